@@ -1,0 +1,266 @@
+/*
+ * sclbm.h -- C ABI of libsclbm_b200.so, a B200 (sm_100a) implementation of the
+ * sc_lbm D2Q9 Shan-Chen time step.
+ *
+ * The reference (LBMFluids/sc_lbm) has no FFI layer: its interface is the C++
+ * classes Geometry / Fluid / LBM.  Every entry point below names the reference
+ * member it replaces (file:line inside the reference project).  The C++
+ * drop-in classes in sc_lbm_b200/host/include/{geometry,fluid,lbm}.h are thin
+ * wrappers over these functions; FFI users (ctypes, cgo, JNI) bind them
+ * directly.
+ *
+ * Conventions (identical to the reference):
+ *   - a lattice is nx * ny nodes, row-major [y*nx + x]; N = nx*ny;
+ *   - masks are int32 per node, 1 = fluid, 0 = solid (Geometry::geom);
+ *   - populations are structure-of-arrays, direction-major [i*N + y*nx + x],
+ *     9 directions with c_x = {0,1,0,-1,0,1,-1,-1,1}, c_y = {0,0,1,0,-1,1,1,-1,-1};
+ *   - every function returns an int status (SCLBM_OK = 0); the C++ layer maps
+ *     the codes to the reference's exception types.  sclbm_last_error() gives
+ *     the message of the last failure on the calling thread;
+ *   - all host pointers are plain host memory (pageable or pinned); device
+ *     state lives inside the opaque handles.  Work is queued on the library
+ *     stream (sclbm_set_stream); functions that return data to the host
+ *     synchronise that stream.
+ */
+#ifndef SCLBM_H
+#define SCLBM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+#define SCLBM_OK 0
+#define SCLBM_E_INVALID_ARGUMENT 1 /* std::invalid_argument in the reference */
+#define SCLBM_E_RUNTIME 2          /* std::runtime_error */
+#define SCLBM_E_OUT_OF_RANGE 3     /* std::out_of_range (vector::at) */
+#define SCLBM_E_DOMAIN 4           /* inputs on which the reference divides by zero */
+#define SCLBM_E_CUDA 5             /* CUDA runtime failure */
+#define SCLBM_E_NO_DEVICE 6        /* no usable CUDA device */
+#define SCLBM_E_NONFINITE 7        /* monitor found NaN/Inf populations */
+#define SCLBM_E_ALLOC 8            /* device allocation failed */
+
+/* Message of the last failure on this thread (always NUL-terminated). */
+int sclbm_last_error(char *buf, size_t len);
+/* Library version string, e.g. "sclbm_b200 0.1.0 sm_100a". */
+const char *sclbm_version(void);
+/* Queue all following work on `cuda_stream` (a cudaStream_t; NULL = the
+ * library's own non-blocking stream). */
+int sclbm_set_stream(void *cuda_stream);
+/* The cudaStream_t in use, as a pointer. */
+void *sclbm_get_stream(void);
+/* Wait for all queued work. */
+int sclbm_synchronize(void);
+
+/* ---------------------------------------------------------------- geometry
+ * Host-side solid mask, bit-exact with the reference Geometry
+ * (include/geometry.h:37-286, src/geometry.cpp). A device copy is made
+ * lazily when an operator first needs it and refreshed after any change. */
+typedef struct sclbm_geometry sclbm_geometry;
+
+/* Geometry::Geometry(Nx, Ny), include/geometry.h:58-59 (all fluid) */
+int sclbm_geometry_create(size_t nx, size_t ny, sclbm_geometry **out);
+void sclbm_geometry_destroy(sclbm_geometry *g);
+int sclbm_geometry_dims(const sclbm_geometry *g, size_t *nx, size_t *ny);
+/* Geometry::add_walls, src/geometry.cpp:34-69 ; where = "x" or "y" */
+int sclbm_geometry_add_walls(sclbm_geometry *g, size_t dH, const char *where);
+/* Geometry::add_rectangle, src/geometry.cpp:76-92 */
+int sclbm_geometry_add_rectangle(sclbm_geometry *g, size_t Lx, size_t Ly, size_t xc, size_t yc);
+/* Geometry::add_square, src/geometry.cpp:95-110 */
+int sclbm_geometry_add_square(sclbm_geometry *g, size_t Ls, size_t xc, size_t yc);
+/* Geometry::add_ellipse, src/geometry.cpp:113-129 */
+int sclbm_geometry_add_ellipse(sclbm_geometry *g, size_t Lx, size_t Ly, size_t xc, size_t yc);
+/* Geometry::add_circle, src/geometry.cpp:132-147 */
+int sclbm_geometry_add_circle(sclbm_geometry *g, size_t D, size_t xc, size_t yc);
+/* Geometry::add_array (displacement overload), src/geometry.cpp:182-198.
+ * bounds = {x_lo, x_hi, y_lo, y_hi}; type is rectangle/square/ellipse/circle. */
+int sclbm_geometry_add_array_spacing(sclbm_geometry *g, const size_t *props, size_t nprops,
+                                     const size_t bounds[4], size_t dx, size_t dy,
+                                     const char *type);
+/* Geometry::add_array (object-number overload), src/geometry.cpp:201-217 */
+int sclbm_geometry_add_array_numbers(sclbm_geometry *g, const size_t *props, size_t nprops,
+                                     const size_t bounds[4], size_t nobj_x, size_t nobj_y,
+                                     const char *type);
+/* Geometry::set_node_fluid / set_node_solid, include/geometry.h:200-210 */
+int sclbm_geometry_set_node(sclbm_geometry *g, size_t x, size_t y, int fluid);
+/* Geometry::get_geom, include/geometry.h:262 (count must be nx*ny) */
+int sclbm_geometry_get_mask(const sclbm_geometry *g, int32_t *mask, size_t count);
+/* Replace the whole mask (Geometry::read's effect, src/geometry.cpp:247-264) */
+int sclbm_geometry_set_mask(sclbm_geometry *g, size_t nx, size_t ny, const int32_t *mask);
+
+/* ------------------------------------------------------------------- fluid
+ * FP64 device state of one component: every array of the reference Fluid
+ * (include/fluid.h:285-309). */
+typedef struct sclbm_fluid sclbm_fluid;
+
+typedef enum {
+    SCLBM_FIELD_F = 0,        /* f_dist, 9N      include/fluid.h:296 */
+    SCLBM_FIELD_FEQ = 1,      /* f_eq_dist, 9N   :298 */
+    SCLBM_FIELD_RHO = 2,      /* rho, N          :303 */
+    SCLBM_FIELD_UX = 3,       /* ux, N           :305 */
+    SCLBM_FIELD_UY = 4,       /* uy, N           :306 */
+    SCLBM_FIELD_UEQ_X = 5,    /* u_eq_x, N       :308 */
+    SCLBM_FIELD_UEQ_Y = 6,    /* u_eq_y, N       :309 */
+    SCLBM_FIELD_FREP_X = 7,   /* F_repulsive_x   :300 */
+    SCLBM_FIELD_FREP_Y = 8,   /* F_repulsive_y   :301 */
+    SCLBM_FIELD_FSOLID_X = 9, /* F_solid_x       :286 */
+    SCLBM_FIELD_FSOLID_Y = 10 /* F_solid_y       :287 */
+} sclbm_field;
+
+/* Fluid(name, cs2, tau) + zero_density_ini: include/fluid.h:60-62,
+ * src/fluid.cpp:43-61.  omega = 1/tau.  All arrays zero; F_solid unset. */
+int sclbm_fluid_create(size_t nx, size_t ny, double tau, sclbm_fluid **out);
+void sclbm_fluid_destroy(sclbm_fluid *f);
+/* Gsolid and Gfluid_repulsion, include/fluid.h:110-114 / src/fluid.cpp:163-168 */
+int sclbm_fluid_set_interactions(sclbm_fluid *f, double g_solid, double g_fluid);
+int sclbm_fluid_get_params(const sclbm_fluid *f, double *omega, double *g_solid, double *g_fluid);
+/* Copy a field host -> device / device -> host (count = 9N or N). Writing
+ * SCLBM_FIELD_FSOLID_X/Y marks the solid force as set (Fluid::add_surface_forces). */
+int sclbm_fluid_write(sclbm_fluid *f, sclbm_field field, const double *src, size_t count);
+int sclbm_fluid_read(sclbm_fluid *f, sclbm_field field, double *dst, size_t count);
+/* Fluid::compute_density, src/fluid.cpp:175-183 */
+int sclbm_fluid_compute_density(sclbm_fluid *f);
+/* Fluid::compute_velocities, src/fluid.cpp:186-200 */
+int sclbm_fluid_compute_velocities(sclbm_fluid *f, const sclbm_geometry *g);
+/* Fluid::compute_f_equilibrium(geom), src/fluid.cpp:210-243 (incl. macroscopic) */
+int sclbm_fluid_compute_f_equilibrium_geom(sclbm_fluid *f, const sclbm_geometry *g);
+/* Fluid::compute_f_equilibrium(), src/fluid.cpp:246-278 */
+int sclbm_fluid_compute_f_equilibrium(sclbm_fluid *f);
+/* Fluid::simple_ini, src/fluid.cpp:64-104: f = rho0/9 on fluid nodes */
+int sclbm_fluid_simple_ini(sclbm_fluid *f, const sclbm_geometry *g, double rho0);
+
+/* --------------------------------------------------------------------- LBM
+ * The step operators of class LBM (include/lbm.h:23-135). Each call launches
+ * sm_100a kernels with the reference's exact FP64 operation order. */
+typedef struct sclbm_lbm sclbm_lbm;
+
+/* LBM::LBM(const Geometry&), include/lbm.h:30-37 (allocates the stream buffer) */
+int sclbm_lbm_create(const sclbm_geometry *g, sclbm_lbm **out);
+void sclbm_lbm_destroy(sclbm_lbm *l);
+/* LBM::initialize_droplet, src/lbm.cpp:11-48 */
+int sclbm_lbm_initialize_droplet(sclbm_lbm *l, const sclbm_geometry *g, sclbm_fluid *bulk,
+                                 sclbm_fluid *droplet, double rho_bulk, double rho_droplet,
+                                 double rho_b_in_d, double rho_d_in_b, double xc, double yc,
+                                 double radius);
+/* LBM::initialize_fluid_rectangle, src/lbm.cpp:51-99 */
+int sclbm_lbm_initialize_fluid_rectangle(sclbm_lbm *l, const sclbm_geometry *g, sclbm_fluid *bulk,
+                                         sclbm_fluid *droplet, double rho_bulk,
+                                         double rho_droplet, double rho_b_in_d,
+                                         double rho_d_in_b, double xc, double yc, double half_lx,
+                                         double half_ly);
+/* The common sums of LBM::compute_solid_surface_force, src/lbm.cpp:102-136,
+ * returned to the host (N each); the C++ layer then applies
+ * Fluid::add_surface_forces (src/fluid.cpp:154-160) to both fluids. */
+int sclbm_lbm_solid_surface_sums(sclbm_lbm *l, const sclbm_geometry *g, double *sx, double *sy,
+                                 size_t count);
+/* LBM::compute_fluid_repulsive_interactions, src/lbm.cpp:144-206 */
+int sclbm_lbm_fluid_repulsive_interactions(sclbm_lbm *l, const sclbm_geometry *g,
+                                           sclbm_fluid *f1, sclbm_fluid *f2);
+/* LBM::compute_equilibrium_velocities, src/lbm.cpp:209-272 (ux/uy receive
+ * momentum, like the reference). Fails with SCLBM_E_OUT_OF_RANGE when a
+ * fluid's solid force was never set, as the reference's .at() does. */
+int sclbm_lbm_equilibrium_velocities(sclbm_lbm *l, const sclbm_geometry *g, sclbm_fluid *f1,
+                                     sclbm_fluid *f2);
+/* LBM::collide(geom, fluid), src/lbm.cpp:275-288 */
+int sclbm_lbm_collide_single(sclbm_lbm *l, const sclbm_geometry *g, sclbm_fluid *f);
+/* LBM::collide(fluid1, fluid2), src/lbm.cpp:291-312 */
+int sclbm_lbm_collide(sclbm_lbm *l, sclbm_fluid *f1, sclbm_fluid *f2);
+/* LBM::add_volume_force (single fluid), src/lbm.cpp:315-325; count >= 9 */
+int sclbm_lbm_add_volume_force_single(sclbm_lbm *l, const sclbm_geometry *g, sclbm_fluid *f,
+                                      const double *force, size_t count);
+/* LBM::add_volume_force (two fluids), src/lbm.cpp:328-340 */
+int sclbm_lbm_add_volume_force(sclbm_lbm *l, const sclbm_geometry *g, sclbm_fluid *f1,
+                               sclbm_fluid *f2, const double *force, size_t count);
+/* LBM::stream(geom, fluid), src/lbm.cpp:343-384 */
+int sclbm_lbm_stream_single(sclbm_lbm *l, const sclbm_geometry *g, sclbm_fluid *f);
+/* LBM::stream(geom, fluid1, fluid2), src/lbm.cpp:387-435 */
+int sclbm_lbm_stream(sclbm_lbm *l, const sclbm_geometry *g, sclbm_fluid *f1, sclbm_fluid *f2);
+
+/* Fused FP64 time steps on fluid objects: each step equals the driver
+ * sequence compute_density x2, compute_fluid_repulsive_interactions,
+ * compute_equilibrium_velocities, collide(f1,f2), add_volume_force (force1 on
+ * f1 and/or force2 on f2 when non-NULL, 9 values each), stream
+ * (laplace_law.cpp:123-133, droplet_in_a_channel.cpp:145-156).  Populations
+ * are bit-identical to that sequence; the intermediate fields (rho, ux, uy,
+ * u_eq, F_repulsive, f_eq) are left as they were. */
+int sclbm_lbm_step(sclbm_lbm *l, const sclbm_geometry *g, sclbm_fluid *f1, sclbm_fluid *f2,
+                   const double *force1, const double *force2, int nsteps);
+/* Fused single-component steps: collide(geom,f), [add_volume_force], stream
+ * (laminar_flow_x_dir.cpp:64-68). */
+int sclbm_lbm_step_single(sclbm_lbm *l, const sclbm_geometry *g, sclbm_fluid *f,
+                          const double *force, int nsteps);
+
+/* ------------------------------------------------------------------ domain
+ * Self-contained device domain for production runs: the mask plus one or two
+ * components in a chosen storage precision, advanced by the fused
+ * single-pass kernel.  No reference counterpart; it runs the same step as
+ * sclbm_lbm_step with the solid force derived from the mask
+ * (LBM::compute_solid_surface_force). */
+typedef enum {
+    SCLBM_FP64 = 0,         /* double storage and arithmetic (bit-exact path) */
+    SCLBM_FP32_SHIFTED = 1, /* float storage of f_i - w_i*rho_ref, float arithmetic */
+    SCLBM_FP16_SHIFTED = 2  /* half storage of f_i - w_i*rho_ref, float arithmetic */
+} sclbm_precision;
+
+typedef struct {
+    int ncomp;          /* 1 or 2 components */
+    double tau[2];      /* relaxation time per component (omega = 1/tau) */
+    double g_fluid[2];  /* Gfluid_repulsion per component */
+    double g_solid[2];  /* Gsolid per component */
+    double rho_ref[2];  /* reference density for the shifted storage */
+    int force_on[2];    /* add force[k] after collision on component k */
+    double force[2][9]; /* volume force per direction (src/lbm.cpp:315-340) */
+} sclbm_params;
+
+typedef struct sclbm_domain sclbm_domain;
+
+int sclbm_domain_create(size_t nx, size_t ny, const int32_t *mask, const sclbm_params *p,
+                        sclbm_precision precision, sclbm_domain **out);
+void sclbm_domain_destroy(sclbm_domain *d);
+/* populations of component comp in reference layout (FP64, 9N values) */
+int sclbm_domain_upload_f(sclbm_domain *d, int comp, const double *f, size_t count);
+int sclbm_domain_download_f(sclbm_domain *d, int comp, double *f, size_t count);
+/* density (Fluid::compute_density) and velocity (Fluid::compute_velocities) */
+int sclbm_domain_download_rho(sclbm_domain *d, int comp, double *rho, size_t count);
+int sclbm_domain_download_velocity(sclbm_domain *d, int comp, double *ux, double *uy,
+                                   size_t count);
+/* advance nsteps time steps (queued on the library stream, not synchronised) */
+int sclbm_domain_step(sclbm_domain *d, int nsteps);
+/* Per component: total mass, x and y momentum over fluid nodes, reduced in
+ * FP64 (out[3*comp + 0..2]); out[6] = number of non-finite populations. */
+int sclbm_domain_mass_momentum(sclbm_domain *d, double out[7]);
+/* Kernel selection: variant 0 = single pass (density recomputed in the
+ * tile), 1 = two pass (density kernel + fused kernel reading it).  tile_y =
+ * rows per tile (0 keeps the default). */
+int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y);
+/* Threads per tile of the two-component kernel: 64, 128 (default) or 256. */
+int sclbm_domain_set_threads(sclbm_domain *d, int tx);
+/* Device bytes held by the domain. */
+size_t sclbm_domain_device_bytes(const sclbm_domain *d);
+/* One end-to-end call: upload both components' populations from host memory,
+ * advance nsteps, return the densities to host memory. f2/rho2 are ignored
+ * for one component. */
+int sclbm_domain_run(sclbm_domain *d, const double *f1, const double *f2, int nsteps,
+                     double *rho1, double *rho2);
+
+/* ------------------------------------------------------------------- batch
+ * Many independent domains of one precision advanced together: one launch
+ * per time step walks a tile list drawn from all domains, and the launch
+ * sequence of a run is captured in a CUDA graph. */
+typedef struct sclbm_batch sclbm_batch;
+
+/* tile_y_per_domain may be NULL (rows per tile chosen by size class) */
+int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *tile_y_per_domain,
+                       sclbm_batch **out);
+void sclbm_batch_destroy(sclbm_batch *b);
+/* advance every domain nsteps; use_graph = 1 replays a captured CUDA graph */
+int sclbm_batch_step(sclbm_batch *b, int nsteps, int use_graph);
+int sclbm_batch_info(const sclbm_batch *b, int *ntiles, int *grid_ctas);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,12 @@
+"""sc_lbm_b200 -- B200-native D2Q9 Shan-Chen lattice-Boltzmann step.
+
+The product is the shared library ``libsclbm_b200.so`` (C ABI in
+include/sclbm.h) with sm_100a kernels, plus the C++ drop-in classes under
+``host/`` (Geometry / Fluid / LBM, same API as LBMFluids/sc_lbm).  This Python
+package is a thin ctypes mirror used by the tests and the benchmark.
+"""
+from .api import LBM, Batch, Domain, Fluid, Geometry, make_params, set_stream, synchronize, version
+from .capi import FP16_SHIFTED, FP32_SHIFTED, FP64
+
+__all__ = ["Geometry", "Fluid", "LBM", "Domain", "Batch", "make_params", "synchronize",
+           "set_stream", "version", "FP64", "FP32_SHIFTED", "FP16_SHIFTED"]

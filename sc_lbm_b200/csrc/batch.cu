@@ -1,0 +1,225 @@
+// batch.cu -- many independent two-component domains advanced together.
+//
+// The work list is every tile (TX-2 columns x tile_y rows) of every domain.
+// One persistent launch per time step walks the list: CTA b takes tiles b,
+// b+grid, b+2*grid, ... with tiles ordered largest-first so the static
+// round-robin stays balanced.  Each tile runs the same fused body as the
+// single-domain kernel (fused2_tile).  The launches of a run are captured once
+// into a CUDA graph and replayed.  All domains of a batch share the storage
+// precision and the buffer parity.
+#include <algorithm>
+#include <numeric>
+
+#include "domain.h"
+#include "fused_step.cuh"
+
+namespace sclbm {
+
+constexpr int BATCH_TX = 128;
+constexpr int GRAPH_STEPS = 20; // launches per captured graph (even: parity returns)
+
+struct TileRef {
+    int dom, xb, yb, pad;
+};
+
+template <typename S, typename T>
+__global__ void __launch_bounds__(BATCH_TX)
+    k_batch2(const Fused2Args<S, T> *__restrict__ doms, const TileRef *__restrict__ tiles, int ntiles,
+             int parity)
+{
+    __shared__ T s_rho[2][4][BATCH_TX];
+    __shared__ uint8_t s_m[4][BATCH_TX];
+    for (int i = blockIdx.x; i < ntiles; i += gridDim.x) {
+        const TileRef tr = tiles[i];
+        Fused2Args<S, T> a = doms[2 * tr.dom + parity]; // argument block of this parity
+        fused2_tile<S, T, BATCH_TX, false>(a, tr.xb, tr.yb, s_rho, s_m);
+        __syncthreads(); // the shared ring is reused by the next tile
+    }
+}
+
+} // namespace sclbm
+
+using namespace sclbm;
+
+struct sclbm_batch {
+    std::vector<sclbm_domain *> doms;
+    sclbm_precision prec = SCLBM_FP32_SHIFTED;
+    void *d_args = nullptr;  // Fused2Args<S,T>[2*ndom] (parity 0, parity 1)
+    TileRef *d_tiles = nullptr;
+    int ntiles = 0, grid = 0, parity = 0;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr}; // by starting parity
+    cudaStream_t graph_stream = nullptr;
+};
+
+template <typename S, typename T>
+static cudaError_t batch_launch(sclbm_batch *b, int parity, cudaStream_t s)
+{
+    k_batch2<S, T><<<b->grid, BATCH_TX, 0, s>>>((const Fused2Args<S, T> *)b->d_args, b->d_tiles,
+                                                 b->ntiles, parity);
+    return cudaGetLastError();
+}
+
+static cudaError_t batch_launch_any(sclbm_batch *b, int parity, cudaStream_t s)
+{
+    switch (b->prec) {
+    case SCLBM_FP64: return batch_launch<double, double>(b, parity, s);
+    case SCLBM_FP32_SHIFTED: return batch_launch<float, float>(b, parity, s);
+    default: return batch_launch<__half, float>(b, parity, s);
+    }
+}
+
+template <typename S, typename T>
+static int upload_args(sclbm_batch *b, const std::vector<int> &ty)
+{
+    std::vector<Fused2Args<S, T>> h(2 * b->doms.size());
+    for (size_t k = 0; k < b->doms.size(); ++k) {
+        sclbm_domain *d = b->doms[k];
+        const int par = d->parity, saved_ty = d->tile_y;
+        d->tile_y = ty[k];
+        for (int p = 0; p < 2; ++p) {
+            d->parity = p;
+            Fused2Args<double, double> a64;
+            Fused2Args<float, float> a32;
+            Fused2Args<__half, float> a16;
+            domain_fused2_args(d, &a64, &a32, &a16);
+            if constexpr (sizeof(S) == 8) h[2 * k + p] = a64;
+            else if constexpr (sizeof(S) == 4) h[2 * k + p] = a32;
+            else h[2 * k + p] = a16;
+        }
+        d->parity = par;
+        d->tile_y = saved_ty;
+    }
+    SCLBM_CUDA(cudaMalloc(&b->d_args, h.size() * sizeof(Fused2Args<S, T>)));
+    SCLBM_CUDA(cudaMemcpy(b->d_args, h.data(), h.size() * sizeof(Fused2Args<S, T>),
+                          cudaMemcpyHostToDevice));
+    return SCLBM_OK;
+}
+
+extern "C" {
+
+void sclbm_batch_destroy(sclbm_batch *b)
+{
+    if (!b) return;
+    for (auto &g : b->graph)
+        if (g) cudaGraphExecDestroy(g);
+    if (b->d_args) cudaFree(b->d_args);
+    if (b->d_tiles) cudaFree(b->d_tiles);
+    delete b;
+}
+
+int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *tile_y_per_domain,
+                       sclbm_batch **out)
+{
+    if (!domains || ndomains < 1 || !out) return set_error(SCLBM_E_INVALID_ARGUMENT, "bad batch");
+    int rc = ensure_device();
+    if (rc) return rc;
+    auto *b = new (std::nothrow) sclbm_batch();
+    if (!b) return set_error(SCLBM_E_ALLOC, "host allocation failed");
+    b->doms.assign(domains, domains + ndomains);
+    b->prec = b->doms[0]->prec;
+    b->parity = b->doms[0]->parity;
+    std::vector<int> ty(ndomains);
+    std::vector<TileRef> tiles;
+    std::vector<long> cost;
+    const int W = BATCH_TX - 2;
+    for (int k = 0; k < ndomains; ++k) {
+        sclbm_domain *d = b->doms[k];
+        if (!d || d->ncomp != 2 || d->prec != b->prec || d->parity != b->parity) {
+            sclbm_batch_destroy(b);
+            return set_error(SCLBM_E_INVALID_ARGUMENT,
+                             "batch domains must be two-component, of one precision and in step");
+        }
+        ty[k] = tile_y_per_domain && tile_y_per_domain[k] > 0 ? tile_y_per_domain[k] : 16;
+        for (int yb = 0; yb < (int)d->ny; yb += ty[k])
+            for (int xb = 0; xb < (int)d->nx; xb += W) {
+                tiles.push_back(TileRef{k, xb, yb, 0});
+                cost.push_back((long)std::min(W, (int)d->nx - xb) * (std::min(ty[k], (int)d->ny - yb) + 2));
+            }
+    }
+    // largest tiles first
+    std::vector<int> order(tiles.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return cost[a] > cost[c]; });
+    std::vector<TileRef> sorted(tiles.size());
+    for (size_t i = 0; i < order.size(); ++i) sorted[i] = tiles[order[i]];
+    b->ntiles = (int)sorted.size();
+    int per_sm = 0;
+    cudaError_t e;
+    switch (b->prec) {
+    case SCLBM_FP64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch2<double, double>, BATCH_TX, 0); break;
+    case SCLBM_FP32_SHIFTED: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch2<float, float>, BATCH_TX, 0); break;
+    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch2<__half, float>, BATCH_TX, 0); break;
+    }
+    if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+    b->grid = std::max(1, std::min(b->ntiles, per_sm * sm_count()));
+    switch (b->prec) {
+    case SCLBM_FP64: rc = upload_args<double, double>(b, ty); break;
+    case SCLBM_FP32_SHIFTED: rc = upload_args<float, float>(b, ty); break;
+    default: rc = upload_args<__half, float>(b, ty); break;
+    }
+    if (!rc && cudaMalloc(&b->d_tiles, sorted.size() * sizeof(TileRef)) != cudaSuccess)
+        rc = set_error(SCLBM_E_CUDA, "tile list allocation");
+    if (!rc && cudaMemcpy(b->d_tiles, sorted.data(), sorted.size() * sizeof(TileRef),
+                          cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = set_error(SCLBM_E_CUDA, "tile list upload");
+    if (rc) {
+        sclbm_batch_destroy(b);
+        return rc;
+    }
+    *out = b;
+    return SCLBM_OK;
+}
+
+int sclbm_batch_info(const sclbm_batch *b, int *ntiles, int *grid_ctas)
+{
+    if (!b) return set_error(SCLBM_E_INVALID_ARGUMENT, "null batch");
+    if (ntiles) *ntiles = b->ntiles;
+    if (grid_ctas) *grid_ctas = b->grid;
+    return SCLBM_OK;
+}
+
+int sclbm_batch_step(sclbm_batch *b, int nsteps, int use_graph)
+{
+    if (!b) return set_error(SCLBM_E_INVALID_ARGUMENT, "null batch");
+    if (nsteps < 0) return set_error(SCLBM_E_INVALID_ARGUMENT, "negative step count");
+    for (auto *d : b->doms)
+        if (d->parity != b->parity)
+            return set_error(SCLBM_E_RUNTIME, "a batch domain was stepped outside the batch");
+    cudaStream_t s = stream();
+    if (use_graph && b->graph_stream != s) {
+        for (auto &g : b->graph)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+        b->graph_stream = s;
+    }
+    int done = 0;
+    while (use_graph && nsteps - done >= GRAPH_STEPS) {
+        cudaGraphExec_t &ge = b->graph[b->parity];
+        if (!ge) {
+            cudaGraph_t g;
+            SCLBM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e = cudaSuccess;
+            for (int k = 0; k < GRAPH_STEPS && e == cudaSuccess; ++k)
+                e = batch_launch_any(b, b->parity ^ (k & 1), s);
+            cudaError_t e2 = cudaStreamEndCapture(s, &g);
+            if (e != cudaSuccess) return cuda_fail(e, "batch capture");
+            if (e2 != cudaSuccess) return cuda_fail(e2, "batch capture end");
+            e = cudaGraphInstantiate(&ge, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");
+        }
+        SCLBM_CUDA(cudaGraphLaunch(ge, s));
+        done += GRAPH_STEPS; // even: parity unchanged
+    }
+    for (; done < nsteps; ++done) {
+        cudaError_t e = batch_launch_any(b, b->parity, s);
+        if (e != cudaSuccess) return cuda_fail(e, "batch step");
+        b->parity ^= 1;
+    }
+    for (auto *d : b->doms) d->parity = b->parity;
+    return SCLBM_OK;
+}
+
+} // extern "C"

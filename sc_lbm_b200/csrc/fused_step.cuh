@@ -1,0 +1,447 @@
+// fused_step.cuh -- the fused Shan-Chen time step (kernel b) and the density
+// pass (kernel a), templated on storage type S and compute type T.
+//
+// One launch performs one complete time step of the reference driver sequence
+//   compute_density x2            src/fluid.cpp:175-183
+//   compute_fluid_repulsive_...   src/lbm.cpp:144-206
+//   compute_equilibrium_velocities src/lbm.cpp:209-272
+//   collide(f1, f2)               src/lbm.cpp:291-312 (+ src/fluid.cpp:246-278)
+//   [add_volume_force]            src/lbm.cpp:315-340
+//   stream(geom, f1, f2)          src/lbm.cpp:387-435
+// reading the populations once and writing them once.
+//
+// Tiling.  A CTA of TX threads owns W = TX-2 interior columns and tile_y rows.
+// Thread t handles column xb-1+t; threads 0 and TX-1 are halo columns that
+// only produce a density.  The CTA marches up its rows: in iteration r it loads
+// row r's populations (kept in registers), reduces them to the density, puts
+// density and mask into a 4-row shared-memory ring, synchronises once, then
+// collides row r-1 using the 3x3 density stencil from the ring and pushes the
+// post-collision populations to their destinations (half-way bounce-back at
+// solid neighbours).  Rows yb-1 and yb+tile_y are halo rows (density only).
+// Every destination slot has exactly one writer, so the kernel is race free
+// with separate input and output buffers.
+//
+// FP64 (EXACT) follows the reference's operation order term by term and is
+// compiled with -fmad=false, so its populations are bit-identical to the
+// serial reference.  The shifted forms (T = float) store d_i = f_i - w_i*rho_ref
+// and evaluate the same physics in deviation form in FP32.
+#pragma once
+#include <cuda_fp16.h>
+
+#include "internal.h"
+#include "lattice.cuh"
+
+namespace sclbm {
+
+template <typename S> struct Store;
+template <> struct Store<double> {
+    static __device__ __forceinline__ double ld(const double *p) { return __ldg(p); }
+    static __device__ __forceinline__ void st(double *p, double v) { *p = v; }
+};
+template <> struct Store<float> {
+    static __device__ __forceinline__ float ld(const float *p) { return __ldg(p); }
+    static __device__ __forceinline__ void st(float *p, float v) { *p = v; }
+};
+template <> struct Store<__half> {
+    static __device__ __forceinline__ float ld(const __half *p) { return __half2float(__ldg(p)); }
+    static __device__ __forceinline__ void st(__half *p, float v) { *p = __float2half_rn(v); }
+};
+
+// equal_floats(r, 0.0, 1e-16) of include/utils.h:145-150
+template <typename T> __device__ __forceinline__ bool rho_is_zero(T r)
+{
+    T a = r < T(0) ? -r : r;
+    T m = T(1);
+    if (m < a) m = a;
+    return a <= T(1e-16) * m;
+}
+
+// ---------------------------------------------------------------------------
+// exact FP64 node update (two components): reference operation order
+// ---------------------------------------------------------------------------
+struct NodeIn2 {
+    double f[2][9];
+};
+
+__device__ __forceinline__ void feq_exact(double r, double ux, double uy, double fe[9])
+{
+    const double rt0 = w_eq(0) * r, rt1 = w_eq(1) * r, rt2 = w_eq(5) * r;
+    const double uxsq = ux * ux, uysq = uy * uy;
+    const double u5 = ux + uy, u6 = -ux + uy, u7 = -ux - uy, u8 = ux - uy;
+    const double usq = uxsq + uysq;
+    fe[0] = rt0 * (1.0 - 1.5 * usq);
+    fe[1] = rt1 * (1.0 + 3.0 * ux + 4.5 * uxsq - 1.5 * usq);
+    fe[2] = rt1 * (1.0 + 3.0 * uy + 4.5 * uysq - 1.5 * usq);
+    fe[3] = rt1 * (1.0 - 3.0 * ux + 4.5 * uxsq - 1.5 * usq);
+    fe[4] = rt1 * (1.0 - 3.0 * uy + 4.5 * uysq - 1.5 * usq);
+    fe[5] = rt2 * (1.0 + 3.0 * u5 + 4.5 * u5 * u5 - 1.5 * usq);
+    fe[6] = rt2 * (1.0 + 3.0 * u6 + 4.5 * u6 * u6 - 1.5 * usq);
+    fe[7] = rt2 * (1.0 + 3.0 * u7 + 4.5 * u7 * u7 - 1.5 * usq);
+    fe[8] = rt2 * (1.0 + 3.0 * u8 + 4.5 * u8 * u8 - 1.5 * usq);
+}
+
+// shifted-form equilibrium deviation: w_i*(drho + rho*(3cu + 4.5cu^2 - 1.5u^2))
+__device__ __forceinline__ float feq_dev(int i, float drho, float r, float ux, float uy, float usq15)
+{
+    const float cu = float(cx(i)) * ux + float(cy(i)) * uy;
+    const float poly = fmaf(cu, fmaf(4.5f, cu, 3.0f), -usq15);
+    return float(w_eq(i)) * fmaf(r, poly, drho);
+}
+
+// ---------------------------------------------------------------------------
+// kernel b: fused two-component step
+// ---------------------------------------------------------------------------
+// One tile: interior columns [xb, xb+W) and rows [yb, yb+tile_y) of domain a.
+template <typename S, typename T, int TX, bool TWO_PASS>
+__device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int xb, const int yb,
+                                            T (&s_rho)[2][4][TX], uint8_t (&s_m)[4][TX])
+{
+    constexpr bool EXACT = sizeof(T) == 8;
+    constexpr int W = TX - 2;
+    const int t = threadIdx.x;
+    const int nx = a.nx, ny = a.ny;
+    const size_t N = a.N;
+    const int ncol = min(W, nx - xb);
+    const int nrow = min(a.tile_y, ny - yb);
+    const bool active = t <= ncol + 1;
+    const bool interior = t >= 1 && t <= ncol;
+    const int x = wrap1(xb - 1 + t, nx);
+    const int xl = wrap1(x - 1, nx), xr = wrap1(x + 1, nx);
+
+    T cur[2][9], prev[2][9];
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+#pragma unroll
+        for (int i = 0; i < 9; ++i) prev[k][i] = cur[k][i] = T(0);
+
+    for (int r = -1; r <= nrow; ++r) {
+        const int y = wrap1(yb + r, ny);
+        const int slot = (r + 1) & 3;
+        T rho[2] = {T(0), T(0)};
+        uint8_t m = 0;
+        if (active) {
+            const size_t node = (size_t)y * nx + x;
+            m = a.mask[node];
+            const bool need_pops = !TWO_PASS || (interior && r >= 0 && r < nrow);
+            if (need_pops) {
+#pragma unroll
+                for (int k = 0; k < 2; ++k)
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) cur[k][i] = T(Store<S>::ld(a.fin[k] + i * N + node));
+            }
+            if (TWO_PASS) {
+                rho[0] = a.rho_in[0][node];
+                rho[1] = a.rho_in[1][node];
+            } else {
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    T s = T(0); // 0.0 + f0 + ... + f8, src/fluid.cpp:177-181
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) s += cur[k][i];
+                    rho[k] = s;
+                }
+            }
+            if (!m) rho[0] = rho[1] = T(0);
+        }
+        s_rho[0][slot][t] = rho[0];
+        s_rho[1][slot][t] = rho[1];
+        s_m[slot][t] = m;
+        __syncthreads();
+
+        if (r >= 1 && interior) {
+            // collide row r-1
+            const int sc = r & 3, sm = (r - 1) & 3, sp = (r + 1) & 3;
+            const int yc = wrap1(yb + r - 1, ny);
+            const int yd = wrap1(yc - 1, ny), yu = wrap1(yc + 1, ny);
+            const size_t node = (size_t)yc * nx + x;
+            if (!s_m[sc][t]) {
+                // solid node: the reference's stream leaves zeros (src/lbm.cpp:431-434)
+#pragma unroll
+                for (int k = 0; k < 2; ++k)
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) Store<S>::st(a.fout[k] + i * N + node, T(0));
+            } else {
+                bool nf[9];
+                T p0[9], p1[9];
+#pragma unroll
+                for (int i = 1; i < 9; ++i) {
+                    const int sl = cy(i) == 0 ? sc : (cy(i) > 0 ? sp : sm);
+                    const int col = t + cx(i);
+                    nf[i] = s_m[sl][col] != 0;
+                    p0[i] = s_rho[0][sl][col];
+                    p1[i] = s_rho[1][sl][col];
+                }
+                const T psi0 = s_rho[0][sc][t], psi1 = s_rho[1][sc][t];
+                T out[2][9];
+                if constexpr (EXACT) {
+                    // repulsive force, src/lbm.cpp:177-204
+                    double F0x = 0.0, F0y = 0.0, F1x = 0.0, F1y = 0.0, Sx = 0.0, Sy = 0.0;
+#pragma unroll
+                    for (int i = 1; i < 9; ++i) {
+                        const double wcx = w_sc(i) * cx(i), wcy = w_sc(i) * cy(i);
+                        if (nf[i]) {
+                            F0x += wcx * p1[i];
+                            F0y += wcy * p1[i];
+                            F1x += wcx * p0[i];
+                            F1y += wcy * p0[i];
+                        } else {
+                            Sx += wcx; // solid sums, src/lbm.cpp:131-134
+                            Sy += wcy;
+                        }
+                    }
+                    F0x *= a.c[0].gf * psi0;
+                    F0y *= a.c[0].gf * psi0;
+                    F1x *= a.c[1].gf * psi1;
+                    F1y *= a.c[1].gf * psi1;
+                    // momentum, src/lbm.cpp:250-255
+                    double j0x = 0.0, j0y = 0.0, j1x = 0.0, j1y = 0.0;
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) {
+                        j0x += prev[0][i] * double(cx(i));
+                        j0y += prev[0][i] * double(cy(i));
+                        j1x += prev[1][i] * double(cx(i));
+                        j1y += prev[1][i] * double(cy(i));
+                    }
+                    const double o0 = a.c[0].omega, o1 = a.c[1].omega;
+                    const double ucx = (j0x * o0 + j1x * o1) / (psi0 * o0 + psi1 * o1);
+                    const double ucy = (j0y * o0 + j1y * o1) / (psi0 * o0 + psi1 * o1);
+                    const double psi[2] = {psi0, psi1};
+                    const double Fx[2] = {F0x, F1x}, Fy[2] = {F0y, F1y};
+#pragma unroll
+                    for (int k = 0; k < 2; ++k) {
+                        double ux, uy;
+                        if (!rho_is_zero(psi[k])) { // src/lbm.cpp:262-269
+                            double fsx, fsy;
+                            if (a.solid_from_mask) {
+                                fsx = a.c[k].gs_neg * Sx;
+                                fsy = a.c[k].gs_neg * Sy;
+                            } else {
+                                fsx = a.fsx[k][node];
+                                fsy = a.fsy[k][node];
+                            }
+                            const double io = a.c[k].inv_omega;
+                            ux = ucx + Fx[k] * io / psi[k] + fsx * io;
+                            uy = ucy + Fy[k] * io / psi[k] + fsy * io;
+                        } else {
+                            ux = a.uex_old[k] ? a.uex_old[k][node] : 0.0;
+                            uy = a.uey_old[k] ? a.uey_old[k][node] : 0.0;
+                        }
+                        double fe[9];
+                        feq_exact(psi[k], ux, uy, fe);
+                        const double om = a.c[k].omega, omm = a.c[k].one_m_omega;
+#pragma unroll
+                        for (int i = 0; i < 9; ++i) {
+                            double v = omm * prev[k][i] + om * fe[i];
+                            if (a.c[k].force_on) v += a.c[k].force[i];
+                            out[k][i] = v;
+                        }
+                    }
+                } else {
+                    // shifted form: s_rho holds rho - rho_ref
+                    float A0x = 0.f, A0y = 0.f, A1x = 0.f, A1y = 0.f, Sx = 0.f, Sy = 0.f;
+#pragma unroll
+                    for (int i = 1; i < 9; ++i) {
+                        const float wcx = float(w_sc(i) * cx(i)), wcy = float(w_sc(i) * cy(i));
+                        if (nf[i]) {
+                            if (cx(i)) { A0x = fmaf(wcx, p1[i], A0x); A1x = fmaf(wcx, p0[i], A1x); }
+                            if (cy(i)) { A0y = fmaf(wcy, p1[i], A0y); A1y = fmaf(wcy, p0[i], A1y); }
+                        } else {
+                            Sx += wcx;
+                            Sy += wcy;
+                        }
+                    }
+                    const float rr0 = a.c[0].rho_ref, rr1 = a.c[1].rho_ref;
+                    const float r0 = rr0 + psi0, r1 = rr1 + psi1;
+                    // sum over fluid neighbours of w c psi = A - rho_ref * S
+                    const float F0x = a.c[0].gf * r0 * fmaf(-rr1, Sx, A0x);
+                    const float F0y = a.c[0].gf * r0 * fmaf(-rr1, Sy, A0y);
+                    const float F1x = a.c[1].gf * r1 * fmaf(-rr0, Sx, A1x);
+                    const float F1y = a.c[1].gf * r1 * fmaf(-rr0, Sy, A1y);
+                    float j0x = (prev[0][1] - prev[0][3]) + (prev[0][5] - prev[0][6]) + (prev[0][8] - prev[0][7]);
+                    float j0y = (prev[0][2] - prev[0][4]) + (prev[0][5] + prev[0][6]) - (prev[0][7] + prev[0][8]);
+                    float j1x = (prev[1][1] - prev[1][3]) + (prev[1][5] - prev[1][6]) + (prev[1][8] - prev[1][7]);
+                    float j1y = (prev[1][2] - prev[1][4]) + (prev[1][5] + prev[1][6]) - (prev[1][7] + prev[1][8]);
+                    const float o0 = a.c[0].omega, o1 = a.c[1].omega;
+                    const float inv_den = 1.0f / fmaf(r0, o0, r1 * o1);
+                    const float ucx = fmaf(j0x, o0, j1x * o1) * inv_den;
+                    const float ucy = fmaf(j0y, o0, j1y * o1) * inv_den;
+                    const float r[2] = {r0, r1}, dr[2] = {psi0, psi1};
+                    const float Fx[2] = {F0x, F1x}, Fy[2] = {F0y, F1y};
+#pragma unroll
+                    for (int k = 0; k < 2; ++k) {
+                        float ux = ucx, uy = ucy;
+                        if (!rho_is_zero(r[k])) {
+                            const float io = a.c[k].inv_omega;
+                            const float ir = io / r[k];
+                            ux = fmaf(Fx[k], ir, fmaf(a.c[k].gs_neg * Sx, io, ucx));
+                            uy = fmaf(Fy[k], ir, fmaf(a.c[k].gs_neg * Sy, io, ucy));
+                        }
+                        const float usq15 = 1.5f * fmaf(ux, ux, uy * uy);
+                        const float om = a.c[k].omega;
+#pragma unroll
+                        for (int i = 0; i < 9; ++i) {
+                            const float fe = feq_dev(i, dr[k], r[k], ux, uy, usq15);
+                            float v = fmaf(om, fe - prev[k][i], prev[k][i]);
+                            if (a.c[k].force_on) v += a.c[k].force[i];
+                            out[k][i] = v;
+                        }
+                    }
+                }
+                // push streaming with half-way bounce-back, src/lbm.cpp:404-427
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    S *o = a.fout[k];
+                    Store<S>::st(o + node, out[k][0]);
+#pragma unroll
+                    for (int i = 1; i < 9; ++i) {
+                        if (nf[i]) {
+                            const int xn = cx(i) == 0 ? x : (cx(i) > 0 ? xr : xl);
+                            const int yn = cy(i) == 0 ? yc : (cy(i) > 0 ? yu : yd);
+                            Store<S>::st(o + i * N + (size_t)yn * nx + xn, out[k][i]);
+                        } else {
+                            Store<S>::st(o + opp(i) * N + node, out[k][i]);
+                        }
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+#pragma unroll
+            for (int i = 0; i < 9; ++i) prev[k][i] = cur[k][i];
+    }
+}
+
+template <typename S, typename T, int TX, bool TWO_PASS>
+__global__ void __launch_bounds__(TX) k_fused2(const __grid_constant__ Fused2Args<S, T> a)
+{
+    __shared__ T s_rho[2][4][TX];
+    __shared__ uint8_t s_m[4][TX];
+    fused2_tile<S, T, TX, TWO_PASS>(a, blockIdx.x * (TX - 2), blockIdx.y * a.tile_y, s_rho, s_m);
+}
+
+// ---------------------------------------------------------------------------
+// single-component fused step: collide(geom,f) + add_volume_force + stream
+// (src/lbm.cpp:275-288, 315-325, 343-384; src/fluid.cpp:175-243)
+// ---------------------------------------------------------------------------
+template <typename S, typename T>
+__global__ void __launch_bounds__(256) k_fused1(const Fused1Args<S, T> a)
+{
+    constexpr bool EXACT = sizeof(T) == 8;
+    const size_t N = a.N;
+    const int nx = a.nx, ny = a.ny;
+    for (size_t node = blockIdx.x * (size_t)blockDim.x + threadIdx.x; node < N;
+         node += (size_t)gridDim.x * blockDim.x) {
+        const int x = int(node % nx), y = int(node / nx);
+        const bool fl = a.mask[node] == 1;
+        if (!fl) {
+#pragma unroll
+            for (int i = 0; i < 9; ++i) Store<S>::st(a.fout + i * N + node, T(0));
+            continue;
+        }
+        T f[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) f[i] = T(Store<S>::ld(a.fin + i * N + node));
+        T out[9];
+        if constexpr (EXACT) {
+            double r = 0.0, ux = 0.0, uy = 0.0;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) r += f[i];
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                ux += f[i] * double(cx(i));
+                uy += f[i] * double(cy(i));
+            }
+            ux /= r;
+            uy /= r;
+            double fe[9];
+            feq_exact(r, ux, uy, fe);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                double v = a.c.one_m_omega * f[i] + a.c.omega * fe[i];
+                if (a.c.force_on) v += a.c.force[i];
+                out[i] = v;
+            }
+        } else {
+            float dr = 0.f;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) dr += f[i];
+            const float r = a.c.rho_ref + dr;
+            const float jx = (f[1] - f[3]) + (f[5] - f[6]) + (f[8] - f[7]);
+            const float jy = (f[2] - f[4]) + (f[5] + f[6]) - (f[7] + f[8]);
+            const float ir = 1.0f / r;
+            const float ux = jx * ir, uy = jy * ir;
+            const float usq15 = 1.5f * fmaf(ux, ux, uy * uy);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                float v = fmaf(a.c.omega, feq_dev(i, dr, r, ux, uy, usq15) - f[i], f[i]);
+                if (a.c.force_on) v += a.c.force[i];
+                out[i] = v;
+            }
+        }
+        const int xl = wrap1(x - 1, nx), xr = wrap1(x + 1, nx);
+        const int yd = wrap1(y - 1, ny), yu = wrap1(y + 1, ny);
+        Store<S>::st(a.fout + node, out[0]);
+#pragma unroll
+        for (int i = 1; i < 9; ++i) {
+            const int xn = cx(i) == 0 ? x : (cx(i) > 0 ? xr : xl);
+            const int yn = cy(i) == 0 ? y : (cy(i) > 0 ? yu : yd);
+            const size_t nb = (size_t)yn * nx + xn;
+            if (a.mask[nb] == 1)
+                Store<S>::st(a.fout + i * N + nb, out[i]);
+            else
+                Store<S>::st(a.fout + opp(i) * N + node, out[i]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// kernel a: density (shifted forms: deviation) of both components, 0 at solids
+// ---------------------------------------------------------------------------
+template <typename S, typename T>
+__global__ void __launch_bounds__(256) k_density2(const uint8_t *__restrict__ mask,
+                                                  const S *__restrict__ f0,
+                                                  const S *__restrict__ f1, T *__restrict__ r0,
+                                                  T *__restrict__ r1, size_t N)
+{
+    for (size_t n = blockIdx.x * (size_t)blockDim.x + threadIdx.x; n < N;
+         n += (size_t)gridDim.x * blockDim.x) {
+        T s0 = T(0), s1 = T(0);
+        if (mask[n]) {
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                s0 += T(Store<S>::ld(f0 + i * N + n));
+                s1 += T(Store<S>::ld(f1 + i * N + n));
+            }
+        }
+        r0[n] = s0;
+        r1[n] = s1;
+    }
+}
+
+template <typename S, typename T, int TX>
+inline cudaError_t launch_fused2_tx(const Fused2Args<S, T> &a, bool two_pass, cudaStream_t s)
+{
+    constexpr int W = TX - 2;
+    dim3 grid((a.nx + W - 1) / W, (a.ny + a.tile_y - 1) / a.tile_y);
+    if (two_pass)
+        k_fused2<S, T, TX, true><<<grid, TX, 0, s>>>(a);
+    else
+        k_fused2<S, T, TX, false><<<grid, TX, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename S, typename T>
+inline cudaError_t launch_fused2_any(const Fused2Args<S, T> &a, int variant, int tx,
+                                     cudaStream_t s)
+{
+    if (a.tile_y < 1 || a.nx < 1 || a.ny < 1) return cudaErrorInvalidValue;
+    const bool two = variant == 1;
+    switch (tx) {
+    case 64: return launch_fused2_tx<S, T, 64>(a, two, s);
+    case 256: return launch_fused2_tx<S, T, 256>(a, two, s);
+    default: return launch_fused2_tx<S, T, 128>(a, two, s);
+    }
+}
+
+} // namespace sclbm

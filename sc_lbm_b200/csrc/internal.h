@@ -1,0 +1,124 @@
+// internal.h -- object layouts and launch entry points shared by the C-ABI
+// translation units of libsclbm_b200.so.  Not installed; the public interface
+// is include/sclbm.h.
+#pragma once
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/sclbm.h"
+
+namespace sclbm {
+
+// ------------------------------------------------------------------ errors
+int set_error(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+#define SCLBM_CUDA(call)                                                                         \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) return ::sclbm::cuda_fail(e_, #call);                              \
+    } while (0)
+#define SCLBM_LAUNCHED(what)                                                                     \
+    do {                                                                                         \
+        cudaError_t e_ = cudaGetLastError();                                                     \
+        if (e_ != cudaSuccess) return ::sclbm::cuda_fail(e_, what);                               \
+    } while (0)
+
+cudaStream_t stream();
+int ensure_device();
+int grid_for(size_t n, int block);  // grid-stride grid size (multiple of the SM count)
+int sm_count();
+
+// ------------------------------------------------------------- host geometry
+int geom_add_walls(std::vector<int32_t> &g, size_t nx, size_t ny, size_t dH, const std::string &w);
+// kind: 0 rectangle, 1 square, 2 ellipse, 3 circle
+int geom_add_object(std::vector<int32_t> &g, size_t nx, size_t ny, int kind, size_t Lx,
+                    size_t Ly, size_t xc, size_t yc);
+int geom_add_array(std::vector<int32_t> &g, size_t nx, size_t ny, const std::string &type,
+                   const size_t *p, size_t np, const size_t *bounds, size_t a, size_t b,
+                   int by_numbers);
+
+} // namespace sclbm
+
+// ------------------------------------------------------------------ objects
+struct sclbm_geometry {
+    size_t nx = 0, ny = 0;
+    std::vector<int32_t> mask; // 1 fluid, 0 solid (Geometry::geom)
+    // lazily refreshed device copy (uint8)
+    mutable uint8_t *d_mask = nullptr;
+    mutable size_t d_count = 0;
+    mutable bool dirty = true;
+};
+
+struct sclbm_fluid {
+    size_t nx = 0, ny = 0, N = 0;
+    double tau = 1.0, omega = 1.0, g_solid = 0.0, g_fluid = 0.0;
+    double *d[11] = {nullptr}; // indexed by sclbm_field
+    bool solid_set = false;
+};
+
+struct sclbm_lbm {
+    size_t nx = 0, ny = 0, N = 0;
+    double *d_tmp[2] = {nullptr, nullptr}; // temp_f_dist, temp_f_dist_spare
+};
+
+namespace sclbm {
+
+// per-component physics constants of the fused kernels (compute type T)
+template <typename T> struct CompParams {
+    T omega, one_m_omega, inv_omega;
+    T gf;      // -1.0 * G  (src/lbm.cpp:163)
+    T gs_neg;  // -1.0 * Gs (src/fluid.cpp:157)
+    T rho_ref; // shift of the stored populations
+    T force[9];
+    int force_on;
+};
+
+// arguments of the two-component fused kernel
+template <typename S, typename T> struct Fused2Args {
+    int nx, ny, tile_y;
+    size_t N;
+    const uint8_t *__restrict__ mask;
+    const S *fin[2];
+    S *fout[2];
+    const double *fsx[2], *fsy[2];       // explicit solid force (FP64 path), or null
+    const double *uex_old[2], *uey_old[2]; // kept u_eq for rho ~ 0 (FP64 path), or null
+    const T *rho_in[2];                  // two-pass variant: density per node
+    CompParams<T> c[2];
+    int solid_from_mask;                 // derive Fs from the mask (domain path)
+};
+
+// arguments of the single-component fused kernel
+template <typename S, typename T> struct Fused1Args {
+    int nx, ny;
+    size_t N;
+    const uint8_t *__restrict__ mask;
+    const S *fin;
+    S *fout;
+    CompParams<T> c;
+};
+
+// launchers implemented in the .cu files; return cudaError_t of the launch
+cudaError_t launch_fused2_fp64(const Fused2Args<double, double> &a, int variant, int tx,
+                               cudaStream_t s);
+cudaError_t launch_fused1_fp64(const Fused1Args<double, double> &a, cudaStream_t s);
+cudaError_t launch_fused2_f32(const Fused2Args<float, float> &a, int variant, int tx,
+                              cudaStream_t s);
+cudaError_t launch_fused1_f32(const Fused1Args<float, float> &a, cudaStream_t s);
+cudaError_t launch_fused2_f16(const Fused2Args<__half, float> &a, int variant, int tx,
+                              cudaStream_t s);
+cudaError_t launch_fused1_f16(const Fused1Args<__half, float> &a, cudaStream_t s);
+// density pass (kernel a): rho (or rho - rho_ref for shifted storage) per node,
+// 0 at solid nodes; both components in one launch
+cudaError_t launch_density_fp64(const uint8_t *mask, const double *f0, const double *f1,
+                                double *r0, double *r1, size_t N, cudaStream_t s);
+cudaError_t launch_density_f32(const uint8_t *mask, const float *f0, const float *f1, float *r0,
+                               float *r1, size_t N, cudaStream_t s);
+cudaError_t launch_density_f16(const uint8_t *mask, const __half *f0, const __half *f1,
+                               float *r0, float *r1, size_t N, cudaStream_t s);
+
+} // namespace sclbm

@@ -1,0 +1,42 @@
+// step_shifted.cu -- FP32 instantiations of the fused step for the shifted
+// storage forms: populations stored as d_i = f_i - w_i*rho_ref in float
+// (SCLBM_FP32_SHIFTED) or half (SCLBM_FP16_SHIFTED), arithmetic in float.
+// Compiled with the default contraction rules (FMA allowed).
+#include "fused_step.cuh"
+
+namespace sclbm {
+
+cudaError_t launch_fused2_f32(const Fused2Args<float, float> &a, int variant, int tx,
+                              cudaStream_t s)
+{
+    return launch_fused2_any<float, float>(a, variant, tx, s);
+}
+cudaError_t launch_fused2_f16(const Fused2Args<__half, float> &a, int variant, int tx,
+                              cudaStream_t s)
+{
+    return launch_fused2_any<__half, float>(a, variant, tx, s);
+}
+cudaError_t launch_fused1_f32(const Fused1Args<float, float> &a, cudaStream_t s)
+{
+    k_fused1<float, float><<<grid_for(a.N, 256), 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t launch_fused1_f16(const Fused1Args<__half, float> &a, cudaStream_t s)
+{
+    k_fused1<__half, float><<<grid_for(a.N, 256), 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t launch_density_f32(const uint8_t *mask, const float *f0, const float *f1, float *r0,
+                               float *r1, size_t N, cudaStream_t s)
+{
+    k_density2<float, float><<<grid_for(N, 256), 256, 0, s>>>(mask, f0, f1, r0, r1, N);
+    return cudaGetLastError();
+}
+cudaError_t launch_density_f16(const uint8_t *mask, const __half *f0, const __half *f1,
+                               float *r0, float *r1, size_t N, cudaStream_t s)
+{
+    k_density2<__half, float><<<grid_for(N, 256), 256, 0, s>>>(mask, f0, f1, r0, r1, N);
+    return cudaGetLastError();
+}
+
+} // namespace sclbm

@@ -1,0 +1,223 @@
+"""GPU parity of libsclbm_b200 against the reference (through the C ABI).
+
+FP64 results are compared BIT FOR BIT with the golden digests recorded from
+the compiled reference (tests/golden/golden_digests.json) and with the CPU
+oracle; the shifted FP32/FP16 storage forms are compared with the FP64 oracle
+within the tolerances stated in each test.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import cases
+import gpu_runner
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+with open(os.path.join(GOLDEN, "golden_digests.json")) as fh:
+    DIGESTS = json.load(fh)["cases"]
+ALL = cases.all_cases()
+SIM = {k: v for k, v in ALL.items() if v["mode"] != "mask"}
+RUNS = {k: v for k, v in SIM.items() if v["mode"] in ("single", "two")}
+
+
+def digest(a):
+    a = np.ascontiguousarray(a)
+    a = a.astype("<f8") if a.dtype.kind == "f" else a.astype("<i4")
+    return hashlib.sha256(a.tobytes()).hexdigest()
+
+
+def assert_golden(name, res, keys=None):
+    want = DIGESTS[name]
+    keys = [k for k in (keys or want) if k in res and k in want]
+    assert keys
+    bad = []
+    for k in keys:
+        if digest(res[k]) != want[k][0]:
+            bad.append(k)
+    assert not bad, f"{name}: differ from the reference: {bad}"
+
+
+# ------------------------------------------------------------------ per operator
+@pytest.mark.parametrize("name", sorted(SIM))
+def test_per_operator_bit_exact(sclbm, name):
+    """One C-ABI call per reference method: every array the reference exposes
+    (f, f_eq, rho, u, u_eq, F_repulsive, F_solid) is bit-identical."""
+    res = gpu_runner.run_ops(sclbm, SIM[name])
+    assert_golden(name, res)
+
+
+# ------------------------------------------------------------------ fused FP64
+@pytest.mark.parametrize("name", sorted(RUNS))
+def test_fused_fp64_bit_exact(sclbm, name):
+    """sclbm_lbm_step / sclbm_lbm_step_single: the single-pass fused kernel
+    reproduces the reference's populations and final macroscopic fields."""
+    res = gpu_runner.run_fused(sclbm, RUNS[name])
+    keys = [k for k in res if k.endswith(("_f", "_final"))]
+    assert_golden(name, res, keys)
+
+
+@pytest.mark.parametrize("name", sorted(RUNS))
+def test_domain_fp64_bit_exact(sclbm, name):
+    res = gpu_runner.run_domain(sclbm, RUNS[name], sclbm.FP64)
+    keys = [k for k in res if k.endswith(("_f", "_final"))]
+    assert_golden(name, res, keys)
+
+
+@pytest.mark.parametrize("tx,tile_y,variant", [(64, 3, 0), (256, 8, 0), (128, 1, 0), (128, 5, 1),
+                                               (64, 64, 1)])
+def test_domain_fp64_tiling_invariant(sclbm, tx, tile_y, variant):
+    """Tile shape and the two-pass variant do not change a single bit."""
+    for name in ("porous_96x48", "spinodal_48x40", "channel_80x32", "droplet_solid_flow"):
+        res = gpu_runner.run_domain(sclbm, RUNS[name], sclbm.FP64, variant=variant,
+                                    tile_y=tile_y, tx=tx)
+        assert_golden(name, res, [k for k in res if k.endswith(("_f", "_final"))])
+
+
+def test_tiny_and_ragged_lattices(sclbm, oracle):
+    """Lattices narrower/shorter than a tile, odd sizes, 1-node-wide periodic wraps."""
+    for nx, ny, geom in ((1, 1, []), (1, 7, []), (5, 1, []), (3, 3, [("walls", 1, "y")]),
+                         (131, 7, [("walls", 1, "x")]), (127, 129, [("circle", 9, 60, 60)])):
+        f = np.concatenate([cases.noisy_f_equilibrium(nx + 3 * ny, nx, ny, 1.0, 0.02, 0.03),
+                            cases.noisy_f_equilibrium(nx + 5 * ny, nx, ny, 0.4, 0.02, 0.03)])
+        case = dict(nx=nx, ny=ny, geom=geom, mode="two", fluid1=(0.9, 1.1, 0.1),
+                    fluid2=(1.2, 1.1, -0.1), init=("file", f),
+                    force=(3, cases.force_vec(1e-4, "x")), steps=7)
+        want = oracle.run_case(case)
+        for runner in (gpu_runner.run_fused,
+                       lambda s, c: gpu_runner.run_domain(s, c, s.FP64, tile_y=2, tx=64)):
+            got = runner(sclbm, case)
+            for k in ("c1_f", "c2_f", "c1_rho_final", "c2_ux_final"):
+                assert got[k].tobytes() == want[k].tobytes(), (nx, ny, k)
+
+
+# ------------------------------------------------------------- shifted forms
+def _rel_err(a, b, mask):
+    m = mask.astype(bool)
+    return np.max(np.abs(a[m] - b[m]) / np.maximum(np.abs(b[m]), 1e-30))
+
+
+@pytest.mark.parametrize("name,prec,tol", [
+    ("spinodal_48x40", "FP32_SHIFTED", 2e-6), ("laplace_64x64", "FP32_SHIFTED", 2e-6),
+    ("porous_96x48", "FP32_SHIFTED", 2e-6), ("channel_80x32", "FP32_SHIFTED", 2e-6),
+    ("poiseuille_200x50", "FP32_SHIFTED", 1e-6),
+    ("spinodal_48x40", "FP16_SHIFTED", 3e-3), ("laplace_64x64", "FP16_SHIFTED", 2e-2),
+    ("porous_96x48", "FP16_SHIFTED", 2e-2), ("poiseuille_200x50", "FP16_SHIFTED", 1e-3)])
+def test_shifted_forms_density_error(sclbm, oracle, name, prec, tol):
+    """Shifted storage (f_i - w_i*rho_ref) with FP32 arithmetic stays within the
+    stated max relative density error of the FP64 oracle on every fluid node."""
+    case = RUNS[name]
+    want = oracle.run_case(case)
+    # rho_ref: the mean initial density of each component
+    f0 = gpu_runner._init_f(case, want["mask"].astype(np.uint8))
+    N = case["nx"] * case["ny"]
+    m = want["mask"].astype(bool)
+    rr = tuple(float(f.reshape(9, N).sum(0)[m].mean()) for f in f0) + (1.0,)
+    got = gpu_runner.run_domain(sclbm, case, getattr(sclbm, prec), rho_ref=rr[:2])
+    for c in ("c1_", "c2_") if case["mode"] == "two" else ("c1_",):
+        err = _rel_err(got[c + "rho_final"], want[c + "rho_final"], want["mask"])
+        assert err <= tol, (name, prec, c, err)
+
+
+def test_shifted_two_pass_matches_single_pass(sclbm):
+    for prec in (sclbm.FP32_SHIFTED, sclbm.FP16_SHIFTED):
+        a = gpu_runner.run_domain(sclbm, RUNS["porous_96x48"], prec, rho_ref=(0.5, 1.5))
+        b = gpu_runner.run_domain(sclbm, RUNS["porous_96x48"], prec, rho_ref=(0.5, 1.5),
+                                  variant=1, tile_y=4)
+        assert a["c1_f"].tobytes() == b["c1_f"].tobytes()
+        assert a["c2_f"].tobytes() == b["c2_f"].tobytes()
+
+
+# ------------------------------------------------------------------- monitors
+def test_mass_momentum_monitor(sclbm):
+    for prec in (sclbm.FP64, sclbm.FP32_SHIFTED, sclbm.FP16_SHIFTED):
+        res = gpu_runner.run_domain(sclbm, RUNS["channel_80x32"], prec, rho_ref=(0.6, 1.4))
+        d = res["_domain"]
+        mm = d.mass_momentum()
+        mask = np.asarray(gpu_runner._geometry(sclbm, RUNS["channel_80x32"])[1], bool)
+        for k in range(2):
+            f = d.download_f(k).reshape(9, -1)[:, mask]
+            assert np.isclose(mm[3 * k], f.sum(), rtol=1e-12)
+            assert np.isclose(mm[3 * k + 1], (cases.CX[:, None] * f).sum(), rtol=1e-9, atol=1e-9)
+            assert np.isclose(mm[3 * k + 2], (cases.CY[:, None] * f).sum(), rtol=1e-9, atol=1e-9)
+        assert mm[6] == 0
+
+
+def test_mass_conserved_in_periodic_domain(sclbm):
+    case = dict(RUNS["spinodal_48x40"], steps=0)
+    for prec, tol in ((sclbm.FP64, 1e-13), (sclbm.FP32_SHIFTED, 1e-6)):
+        d = gpu_runner.make_domain(sclbm, case, prec)
+        m0 = d.mass_momentum()
+        d.step(500)
+        m1 = d.mass_momentum()
+        for k in range(2):
+            assert abs(m1[3 * k] - m0[3 * k]) <= tol * abs(m0[3 * k]), (prec, k)
+
+
+def test_monitor_reports_non_finite(sclbm):
+    case = dict(RUNS["spinodal_48x40"], steps=0)
+    d = gpu_runner.make_domain(sclbm, case, sclbm.FP64)
+    f = d.download_f(0)
+    f[5] = np.nan
+    d.upload_f(0, f)
+    from sc_lbm_b200.capi import SclbmNonFinite
+    with pytest.raises(SclbmNonFinite):
+        d.mass_momentum()
+
+
+# ---------------------------------------------------------------------- batch
+def test_batch_matches_individual_domains(sclbm):
+    names = ["porous_96x48", "spinodal_48x40", "channel_80x32", "laplace_64x64",
+             "droplet_solid_flow", "absent_24x16"]
+    for prec, graph in ((sclbm.FP64, True), (sclbm.FP32_SHIFTED, True), (sclbm.FP16_SHIFTED, False)):
+        rr = (0.8, 1.2)
+        solo = [gpu_runner.run_domain(sclbm, dict(RUNS[n], steps=45), prec, rho_ref=rr) for n in names]
+        doms = [gpu_runner.make_domain(sclbm, RUNS[n], prec, rho_ref=rr) for n in names]
+        b = sclbm.Batch(doms, tile_y=[3, 16, 8, 5, 12, 2])
+        b.step(45, use_graph=graph)
+        for s, d, n in zip(solo, doms, names):
+            for k in range(2):
+                assert d.download_f(k).tobytes() == s[f"c{k + 1}_f"].tobytes(), (prec, n, k)
+
+
+def test_batch_fp64_matches_reference(sclbm):
+    names = ["porous_96x48", "spinodal_48x40", "laplace_64x64"]
+    doms = [gpu_runner.make_domain(sclbm, RUNS[n], sclbm.FP64) for n in names]
+    steps = {RUNS[n]["steps"] for n in names}
+    doms_by = {}
+    for n, d in zip(names, doms):
+        doms_by.setdefault(RUNS[n]["steps"], []).append((n, d))
+    for st, group in doms_by.items():
+        b = sclbm.Batch([d for _, d in group])
+        b.step(st, use_graph=True)
+        for n, d in group:
+            res = {"c1_f": d.download_f(0), "c2_f": d.download_f(1)}
+            assert_golden(n, res, ["c1_f", "c2_f"])
+    assert steps
+
+
+# ----------------------------------------------------------------- error paths
+def test_reference_error_behaviour(sclbm):
+    g = sclbm.Geometry(10, 8)
+    a, b = sclbm.Fluid(g), sclbm.Fluid(g)
+    lbm = sclbm.LBM(g)
+    # compute_equilibrium_velocities before the solid force exists: out_of_range
+    with pytest.raises(IndexError):
+        lbm.compute_equilibrium_velocities(g, a, b)
+    with pytest.raises(IndexError):
+        lbm.add_volume_force(g, a, [0.0] * 8)
+    g2 = sclbm.Geometry(11, 8)
+    with pytest.raises(ValueError):
+        lbm.stream(g2, sclbm.Fluid(g2))
+    bad = g.get_geom()
+    bad[3] = 2
+    with pytest.raises(ValueError):
+        sclbm.Domain(10, 8, bad, sclbm.make_params())
+    with pytest.raises(ValueError):
+        sclbm.Domain(10, 8, g.get_geom(), sclbm.make_params(tau=(0.0, 1.0)))
+    with pytest.raises(IndexError):
+        lbm.initialize_fluid_rectangle(g, a, b, 2.0, 2.0, 0.1, 0.1, 9.0, 6.0, 5.0, 3.0)

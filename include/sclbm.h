@@ -232,9 +232,13 @@ int sclbm_domain_step(sclbm_domain *d, int nsteps);
 /* Per component: total mass, x and y momentum over fluid nodes, reduced in
  * FP64 (out[3*comp + 0..2]); out[6] = number of non-finite populations. */
 int sclbm_domain_mass_momentum(sclbm_domain *d, double out[7]);
-/* Kernel selection: variant 0 = single pass (density recomputed in the
- * tile), 1 = two pass (density kernel + fused kernel reading it).  tile_y =
- * rows per tile (0 keeps the default). */
+/* Kernel selection (all variants give identical FP64 results):
+ *   0 = single pass, persistent and load-balanced, population rows staged
+ *       through a shared-memory ring by asynchronous copies (default; the
+ *       FP16 form falls back to 2);
+ *   1 = two pass (density kernel, then the fused kernel reading it);
+ *   2 = single pass, one tile per CTA, rows held in registers.
+ * tile_y = rows per tile of variants 1 and 2 (0 keeps the default). */
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y);
 /* Threads per tile of the two-component kernel: 64, 128 (default) or 256. */
 int sclbm_domain_set_threads(sclbm_domain *d, int tx);
@@ -256,6 +260,9 @@ typedef struct sclbm_batch sclbm_batch;
 int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *tile_y_per_domain,
                        sclbm_batch **out);
 void sclbm_batch_destroy(sclbm_batch *b);
+/* Work decomposition: 0 = balanced row units over all domains (default for
+ * FP64/FP32 storage), 2 = tile list with tile_y rows per tile (FP16). */
+int sclbm_batch_set_kernel(sclbm_batch *b, int variant);
 /* advance every domain nsteps; use_graph = 1 replays a captured CUDA graph */
 int sclbm_batch_step(sclbm_batch *b, int nsteps, int use_graph);
 int sclbm_batch_info(const sclbm_batch *b, int *ntiles, int *grid_ctas);

@@ -304,6 +304,9 @@ class Batch(_Handle):
     def step(self, n=1, use_graph=True):
         call("sclbm_batch_step", self._h, int(n), 1 if use_graph else 0)
 
+    def set_kernel(self, variant):
+        call("sclbm_batch_set_kernel", self._h, int(variant))
+
     def info(self):
         a, b = C.c_int(), C.c_int()
         call("sclbm_batch_info", self._h, C.byref(a), C.byref(b))

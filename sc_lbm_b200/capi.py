@@ -119,6 +119,7 @@ SIGNATURES = {
     "sclbm_batch_create": (C.c_int, [C.POINTER(_VP), C.c_int, C.POINTER(C.c_int), C.POINTER(_VP)]),
     "sclbm_batch_destroy": (None, [_VP]),
     "sclbm_batch_step": (C.c_int, [_VP, C.c_int, C.c_int]),
+    "sclbm_batch_set_kernel": (C.c_int, [_VP, C.c_int]),
     "sclbm_batch_info": (C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
 }
 

@@ -1,70 +1,58 @@
-// batch.cu -- many independent two-component domains advanced together.
+// batch.cu -- many independent two-component domains advanced together, one
+// persistent launch per time step, the launches of a run captured once into a
+// CUDA graph and replayed.  All domains of a batch share the storage precision
+// and the buffer parity.  Two work decompositions:
 //
-// The work list is every tile (TX-2 columns x tile_y rows) of every domain.
-// One persistent launch per time step walks the list: CTA b takes tiles b,
-// b+grid, b+2*grid, ... with tiles ordered largest-first so the static
-// round-robin stays balanced.  Each tile runs the same fused body as the
-// single-domain kernel (fused2_tile).  The launches of a run are captured once
-// into a CUDA graph and replayed.  All domains of a batch share the storage
-// precision and the buffer parity.
+//  * units (default for FP64/FP32): the rows of the 128-column strips of all
+//    domains are concatenated and cut into equal contiguous chunks, one per
+//    resident CTA (fused_async.cuh); balanced to a row whatever the domain
+//    sizes;
+//  * tile list (FP16, or on request): every tile (126 columns x tile_y rows)
+//    of every domain, largest first; CTA b takes tiles b, b+grid, ... and runs
+//    the register-tile body (batch_kernel.cuh).
 #include <algorithm>
 #include <numeric>
 
 #include "domain.h"
-#include "fused_step.cuh"
+#include "batch_kernel.cuh"
 
-namespace sclbm {
-
-constexpr int BATCH_TX = 128;
-constexpr int GRAPH_STEPS = 20; // launches per captured graph (even: parity returns)
-
-struct TileRef {
-    int dom, xb, yb, pad;
-};
-
-template <typename S, typename T>
-__global__ void __launch_bounds__(BATCH_TX)
-    k_batch2(const Fused2Args<S, T> *__restrict__ doms, const TileRef *__restrict__ tiles, int ntiles,
-             int parity)
-{
-    __shared__ T s_rho[2][4][BATCH_TX];
-    __shared__ uint8_t s_m[4][BATCH_TX];
-    for (int i = blockIdx.x; i < ntiles; i += gridDim.x) {
-        const TileRef tr = tiles[i];
-        Fused2Args<S, T> a = doms[2 * tr.dom + parity]; // argument block of this parity
-        fused2_tile<S, T, BATCH_TX, false>(a, tr.xb, tr.yb, s_rho, s_m);
-        __syncthreads(); // the shared ring is reused by the next tile
-    }
-}
-
-} // namespace sclbm
 
 using namespace sclbm;
+
+static constexpr int GRAPH_STEPS = 20; // launches per captured graph (even: parity returns)
 
 struct sclbm_batch {
     std::vector<sclbm_domain *> doms;
     sclbm_precision prec = SCLBM_FP32_SHIFTED;
     void *d_args = nullptr;  // Fused2Args<S,T>[2*ndom] (parity 0, parity 1)
     TileRef *d_tiles = nullptr;
+    long long *d_prefix = nullptr; // first unit of each domain, then the total
+    long long units = 0;
     int ntiles = 0, grid = 0, parity = 0;
+    int use_units = 1;
     cudaGraphExec_t graph[2] = {nullptr, nullptr}; // by starting parity
     cudaStream_t graph_stream = nullptr;
 };
 
-template <typename S, typename T>
-static cudaError_t batch_launch(sclbm_batch *b, int parity, cudaStream_t s)
-{
-    k_batch2<S, T><<<b->grid, BATCH_TX, 0, s>>>((const Fused2Args<S, T> *)b->d_args, b->d_tiles,
-                                                 b->ntiles, parity);
-    return cudaGetLastError();
-}
-
 static cudaError_t batch_launch_any(sclbm_batch *b, int parity, cudaStream_t s)
 {
+    const int nd = (int)b->doms.size();
+    if (b->use_units && b->prec == SCLBM_FP64)
+        return launch_batch2_async_fp64((const Fused2Args<double, double> *)b->d_args, b->d_prefix,
+                                        nd, b->units, parity, s);
+    if (b->use_units && b->prec == SCLBM_FP32_SHIFTED)
+        return launch_batch2_async_f32((const Fused2Args<float, float> *)b->d_args, b->d_prefix,
+                                       nd, b->units, parity, s);
     switch (b->prec) {
-    case SCLBM_FP64: return batch_launch<double, double>(b, parity, s);
-    case SCLBM_FP32_SHIFTED: return batch_launch<float, float>(b, parity, s);
-    default: return batch_launch<__half, float>(b, parity, s);
+    case SCLBM_FP64:
+        return launch_batch_fp64((const Fused2Args<double, double> *)b->d_args, b->d_tiles,
+                                 b->ntiles, parity, b->grid, s);
+    case SCLBM_FP32_SHIFTED:
+        return launch_batch_f32((const Fused2Args<float, float> *)b->d_args, b->d_tiles,
+                                b->ntiles, parity, b->grid, s);
+    default:
+        return launch_batch_f16((const Fused2Args<__half, float> *)b->d_args, b->d_tiles,
+                                b->ntiles, parity, b->grid, s);
     }
 }
 
@@ -104,6 +92,7 @@ void sclbm_batch_destroy(sclbm_batch *b)
         if (g) cudaGraphExecDestroy(g);
     if (b->d_args) cudaFree(b->d_args);
     if (b->d_tiles) cudaFree(b->d_tiles);
+    if (b->d_prefix) cudaFree(b->d_prefix);
     delete b;
 }
 
@@ -143,20 +132,26 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
     std::vector<TileRef> sorted(tiles.size());
     for (size_t i = 0; i < order.size(); ++i) sorted[i] = tiles[order[i]];
     b->ntiles = (int)sorted.size();
-    int per_sm = 0;
-    cudaError_t e;
-    switch (b->prec) {
-    case SCLBM_FP64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch2<double, double>, BATCH_TX, 0); break;
-    case SCLBM_FP32_SHIFTED: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch2<float, float>, BATCH_TX, 0); break;
-    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch2<__half, float>, BATCH_TX, 0); break;
-    }
-    if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+    int per_sm = batch_blocks_per_sm(b->prec);
+    if (per_sm < 1) per_sm = 1;
     b->grid = std::max(1, std::min(b->ntiles, per_sm * sm_count()));
     switch (b->prec) {
     case SCLBM_FP64: rc = upload_args<double, double>(b, ty); break;
     case SCLBM_FP32_SHIFTED: rc = upload_args<float, float>(b, ty); break;
     default: rc = upload_args<__half, float>(b, ty); break;
     }
+    std::vector<long long> prefix(ndomains + 1, 0);
+    for (int k = 0; k < ndomains; ++k) {
+        const sclbm_domain *d = b->doms[k];
+        prefix[k + 1] = prefix[k] + (long long)((d->nx + ASYNC_STRIP - 1) / ASYNC_STRIP) * d->ny;
+    }
+    b->units = prefix[ndomains];
+    b->use_units = b->prec != SCLBM_FP16_SHIFTED;
+    if (!rc && cudaMalloc(&b->d_prefix, prefix.size() * sizeof(long long)) != cudaSuccess)
+        rc = set_error(SCLBM_E_CUDA, "unit prefix allocation");
+    if (!rc && cudaMemcpy(b->d_prefix, prefix.data(), prefix.size() * sizeof(long long),
+                          cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = set_error(SCLBM_E_CUDA, "unit prefix upload");
     if (!rc && cudaMalloc(&b->d_tiles, sorted.size() * sizeof(TileRef)) != cudaSuccess)
         rc = set_error(SCLBM_E_CUDA, "tile list allocation");
     if (!rc && cudaMemcpy(b->d_tiles, sorted.data(), sorted.size() * sizeof(TileRef),
@@ -167,6 +162,21 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
         return rc;
     }
     *out = b;
+    return SCLBM_OK;
+}
+
+int sclbm_batch_set_kernel(sclbm_batch *b, int variant)
+{
+    if (!b) return set_error(SCLBM_E_INVALID_ARGUMENT, "null batch");
+    if (variant != 0 && variant != 2) return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0 or 2");
+    if (variant == 0 && b->prec == SCLBM_FP16_SHIFTED)
+        return set_error(SCLBM_E_INVALID_ARGUMENT, "the FP16 form uses the tile list (variant 2)");
+    b->use_units = variant == 0;
+    for (auto &g : b->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
     return SCLBM_OK;
 }
 

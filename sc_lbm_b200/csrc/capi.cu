@@ -698,7 +698,7 @@ int sclbm_lbm_step(sclbm_lbm *l, const sclbm_geometry *g, sclbm_fluid *f1, sclbm
         a.fin[1] = f2->d[SCLBM_FIELD_F];
         a.fout[0] = l->d_tmp[0];
         a.fout[1] = l->d_tmp[1];
-        CUDA_LAUNCH(launch_fused2_fp64(a, 0, 128, stream()));
+        CUDA_LAUNCH(launch_fused2_async_fp64(a, stream()));
         std::swap(f1->d[SCLBM_FIELD_F], l->d_tmp[0]);
         std::swap(f2->d[SCLBM_FIELD_F], l->d_tmp[1]);
     }

@@ -251,9 +251,15 @@ static cudaError_t step_one(const sclbm_domain *d, cudaStream_t s)
                                    (float *)d->rho_tmp[1], d->N, s);
         if (e != cudaSuccess) return e;
     }
-    if constexpr (sizeof(S) == 8) return launch_fused2_fp64(a, d->variant, d->tx, s);
-    else if constexpr (sizeof(S) == 4) return launch_fused2_f32(a, d->variant, d->tx, s);
-    else return launch_fused2_f16(a, d->variant, d->tx, s);
+    if (d->variant == 0) { // pipelined persistent single pass (FP64 / FP32 storage)
+        if constexpr (sizeof(S) == 8) return launch_fused2_async_fp64(a, s);
+        else if constexpr (sizeof(S) == 4) return launch_fused2_async_f32(a, s);
+    }
+    // variant 1: two pass; variant 2 (and FP16): register-tile single pass
+    const int v = d->variant == 1 ? 1 : 0;
+    if constexpr (sizeof(S) == 8) return launch_fused2_fp64(a, v, d->tx, s);
+    else if constexpr (sizeof(S) == 4) return launch_fused2_f32(a, v, d->tx, s);
+    else return launch_fused2_f16(a, v, d->tx, s);
 }
 
 int domain_launch_step(sclbm_domain *d, cudaStream_t s)
@@ -359,7 +365,7 @@ fail:
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y)
 {
     if (!d) return set_error(SCLBM_E_INVALID_ARGUMENT, "null domain");
-    if (variant != 0 && variant != 1) return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0 or 1");
+    if (variant < 0 || variant > 2) return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0, 1 or 2");
     if (tile_y < 0 || tile_y > 4096) return set_error(SCLBM_E_INVALID_ARGUMENT, "bad tile_y");
     if (variant == 1 && !d->rho_tmp[0] && d->ncomp == 2) {
         const size_t es = d->prec == SCLBM_FP64 ? 8 : 4;

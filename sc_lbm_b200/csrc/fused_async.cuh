@@ -1,0 +1,229 @@
+// fused_async.cuh -- persistent, load-balanced variant of the fused step with
+// the population rows staged through a shared-memory ring by asynchronous
+// global->shared copies (cp.async / LDGSTS).
+//
+// Work decomposition.  The lattice is cut into column strips of TX columns
+// (one thread per column, all threads interior); a "unit" is one row of one
+// strip.  The U = strips x ny units are split into gridDim.x contiguous,
+// equal chunks, one per CTA, and the grid is sized to the number of CTAs
+// that are resident at once, so every SM finishes together (no tail wave).
+// A chunk is processed as one or more segments (a run of rows inside one
+// strip); each segment reads two halo rows and two halo columns.
+//
+// Pipeline.  For a segment, local row lr (0 = the halo row below, nrow+1 =
+// the halo row above) lives in ring stage lr % R.  Before the row loop, rows
+// 0..R-2 are requested; iteration lr waits for row lr, reduces it to the
+// densities of both components (shared density ring, one __syncthreads),
+// collides row lr-1 from its populations still in the ring, pushes the
+// results to global memory, and finally requests row lr+R-1 into the stage
+// that row lr-1 just vacated.  Each thread copies and reads only its own
+// column (threads 0 and ncol-1 also the halo columns), so the population ring
+// needs no barrier; R-1 rows per thread are in flight while it computes.
+#pragma once
+#include <cuda_pipeline.h>
+
+#include "fused_step.cuh"
+
+namespace sclbm {
+
+template <typename S, typename T, int TX, int R> struct AsyncLayout {
+    static constexpr int P = TX + 2; // columns including the two halo columns
+    static constexpr size_t pops = size_t(R) * 18 * P * sizeof(S);
+    static constexpr size_t rho = size_t(2) * 4 * P * sizeof(T);
+    static constexpr size_t bytes = pops + rho + 4 * P;
+};
+
+template <typename S, typename T, int TX, int R>
+__device__ __forceinline__ void async_copy_node(S *pops, int stage, int col,
+                                                const Fused2Args<S, T> &a, size_t node)
+{
+    constexpr int P = TX + 2;
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+            __pipeline_memcpy_async(pops + ((stage * 2 + k) * 9 + i) * P + col,
+                                    a.fin[k] + i * a.N + node, sizeof(S));
+}
+
+template <typename S, typename T, int TX, int R>
+__device__ __forceinline__ void async_density(const S *pops, int stage, int col, uint8_t m,
+                                              T *rho, uint8_t *msk, int slot)
+{
+    constexpr int P = TX + 2;
+    T r[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        T s = T(0); // 0.0 + f0 + ... + f8, src/fluid.cpp:177-181
+#pragma unroll
+        for (int i = 0; i < 9; ++i) s += T(pops[((stage * 2 + k) * 9 + i) * P + col]);
+        r[k] = m ? s : T(0);
+    }
+    rho[(0 * 4 + slot) * P + col] = r[0];
+    rho[(1 * 4 + slot) * P + col] = r[1];
+    msk[slot * P + col] = m;
+}
+
+// Rows [y0, y1) of the strip starting at column xb.
+template <typename S, typename T, int TX, int R>
+__device__ __forceinline__ void async_segment(const Fused2Args<S, T> &a, const int xb,
+                                              const int y0, const int y1, unsigned char *smem)
+{
+    using L = AsyncLayout<S, T, TX, R>;
+    constexpr int P = L::P;
+    S *pops = reinterpret_cast<S *>(smem);
+    T *rho = reinterpret_cast<T *>(smem + L::pops);
+    uint8_t *msk = smem + L::pops + L::rho;
+
+    const int t = threadIdx.x;
+    const int nx = a.nx, ny = a.ny;
+    const int ncol = min(TX, nx - xb);
+    const int nrow = y1 - y0;
+    const bool act = t < ncol;
+    const bool hl = act && t == 0, hr = act && t == ncol - 1;
+    const int x = act ? xb + t : 0;
+    const int xl = wrap1(x - 1, nx), xr = wrap1(x + 1, nx);
+    const int xhl = wrap1(xb - 1, nx), xhr = wrap1(xb + ncol, nx);
+    const int last = nrow + 1;
+
+    int issue_stage = 0;
+    auto issue = [&](int lr) {
+        if (act && lr <= last) {
+            const size_t row = (size_t)wrap1(y0 - 1 + lr, ny) * nx;
+            async_copy_node<S, T, TX, R>(pops, issue_stage, t + 1, a, row + x);
+            if (hl) async_copy_node<S, T, TX, R>(pops, issue_stage, 0, a, row + xhl);
+            if (hr) async_copy_node<S, T, TX, R>(pops, issue_stage, ncol + 1, a, row + xhr);
+        }
+        __pipeline_commit();
+        issue_stage = issue_stage + 1 == R ? 0 : issue_stage + 1;
+    };
+#pragma unroll
+    for (int q = 0; q < R - 1; ++q) issue(q);
+
+    uint8_t mn = 0, mnl = 0, mnr = 0; // masks of the next row (loaded one row ahead)
+    if (act) {
+        const size_t row = (size_t)wrap1(y0 - 1, ny) * nx;
+        mn = a.mask[row + x];
+        if (hl) mnl = a.mask[row + xhl];
+        if (hr) mnr = a.mask[row + xhr];
+    }
+    int stage = 0;                     // ring stage of row lr
+    int cstage = R - 1;                // ring stage of row lr-1
+    for (int lr = 0; lr <= last; ++lr) {
+        const int slot = lr & 3;
+        const uint8_t m = mn, ml = mnl, mr = mnr;
+        if (act && lr < last) {
+            const size_t row = (size_t)wrap1(y0 + lr, ny) * nx;
+            mn = a.mask[row + x];
+            if (hl) mnl = a.mask[row + xhl];
+            if (hr) mnr = a.mask[row + xhr];
+        }
+        __pipeline_wait_prior(R - 2);
+        if (act) {
+            async_density<S, T, TX, R>(pops, stage, t + 1, m, rho, msk, slot);
+            if (hl) async_density<S, T, TX, R>(pops, stage, 0, ml, rho, msk, slot);
+            if (hr) async_density<S, T, TX, R>(pops, stage, ncol + 1, mr, rho, msk, slot);
+        }
+        __syncthreads();
+        if (act && lr >= 2) {
+            const int yc = wrap1(y0 + lr - 2, ny);
+            const int yd = wrap1(yc - 1, ny), yu = wrap1(yc + 1, ny);
+            const int sm = (lr - 2) & 3, sc = (lr - 1) & 3, sp = slot;
+            const RingPops<S, T, P> f{pops + cstage * 18 * P + t + 1};
+            const Stencil<T> st{{rho + (0 * 4 + sm) * P, rho + (0 * 4 + sc) * P, rho + (0 * 4 + sp) * P},
+                                {rho + (1 * 4 + sm) * P, rho + (1 * 4 + sc) * P, rho + (1 * 4 + sp) * P},
+                                {msk + sm * P, msk + sc * P, msk + sp * P}, t + 1};
+            collide_push<S, T>(a, f, st, x, xl, xr, yc, yd, yu);
+        }
+        // row lr-1's stage is free again: request row lr+R-1 into it
+        issue(lr + R - 1);
+        cstage = stage;
+        stage = stage + 1 == R ? 0 : stage + 1;
+    }
+    __pipeline_wait_prior(0);
+    __syncthreads(); // the rings are reused by the next segment
+}
+
+template <typename S, typename T, int TX, int R>
+__global__ void __launch_bounds__(TX) k_fused2_async(const __grid_constant__ Fused2Args<S, T> a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int nstrips = (a.nx + TX - 1) / TX;
+    const long long U = (long long)nstrips * a.ny;
+    const long long u0 = U * blockIdx.x / gridDim.x, u1 = U * (blockIdx.x + 1) / gridDim.x;
+    for (long long u = u0; u < u1;) {
+        const int s = int(u / a.ny), y0 = int(u % a.ny);
+        const int y1 = (int)min((long long)a.ny, (long long)y0 + (u1 - u));
+        async_segment<S, T, TX, R>(a, s * TX, y0, y1, smem);
+        u += y1 - y0;
+    }
+}
+
+// Batched form: the units of all domains are concatenated (prefix[d] = first
+// unit of domain d, prefix[ndom] = total) and split the same way.
+template <typename S, typename T, int TX, int R>
+__global__ void __launch_bounds__(TX)
+    k_batch2_async(const Fused2Args<S, T> *__restrict__ doms, const long long *__restrict__ prefix,
+                   int ndom, int parity)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const long long U = prefix[ndom];
+    const long long u0 = U * blockIdx.x / gridDim.x, u1 = U * (blockIdx.x + 1) / gridDim.x;
+    int lo = 0, hi = ndom - 1; // last domain with prefix[d] <= u0
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= u0) lo = mid;
+        else hi = mid - 1;
+    }
+    int d = lo;
+    for (long long u = u0; u < u1;) {
+        while (prefix[d + 1] <= u) ++d;
+        const Fused2Args<S, T> a = doms[2 * d + parity];
+        const long long local = u - prefix[d];
+        const int s = int(local / a.ny), y0 = int(local % a.ny);
+        const int y1 = (int)min((long long)a.ny, (long long)y0 + (u1 - u));
+        async_segment<S, T, TX, R>(a, s * TX, y0, y1, smem);
+        u += y1 - y0;
+    }
+}
+
+// resident CTAs per SM for a kernel with the ring's dynamic shared memory
+template <typename K> inline int resident_ctas(K kernel, int threads, size_t smem)
+{
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+        return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess)
+        return 0;
+    return n;
+}
+
+template <typename S, typename T, int TX, int R>
+inline cudaError_t launch_fused2_async_t(const Fused2Args<S, T> &a, cudaStream_t s)
+{
+    using L = AsyncLayout<S, T, TX, R>;
+    static int per_sm = resident_ctas(k_fused2_async<S, T, TX, R>, TX, L::bytes);
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    const long long U = (long long)((a.nx + TX - 1) / TX) * a.ny;
+    long long grid = (long long)per_sm * sm_count();
+    grid = std::max(1LL, std::min(grid, U / 4));
+    k_fused2_async<S, T, TX, R><<<(int)grid, TX, L::bytes, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename S, typename T, int TX, int R>
+inline cudaError_t launch_batch2_async_t(const Fused2Args<S, T> *doms, const long long *prefix,
+                                         int ndom, long long units, int parity, cudaStream_t s)
+{
+    using L = AsyncLayout<S, T, TX, R>;
+    static int per_sm = resident_ctas(k_batch2_async<S, T, TX, R>, TX, L::bytes);
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    long long grid = (long long)per_sm * sm_count();
+    grid = std::max(1LL, std::min(grid, units / 4));
+    k_batch2_async<S, T, TX, R><<<(int)grid, TX, L::bytes, s>>>(doms, prefix, ndom, parity);
+    return cudaGetLastError();
+}
+
+} // namespace sclbm

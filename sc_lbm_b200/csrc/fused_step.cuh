@@ -88,6 +88,195 @@ __device__ __forceinline__ float feq_dev(int i, float drho, float r, float ux, f
     return float(w_eq(i)) * fmaf(r, poly, drho);
 }
 
+// Density/mask stencil around one node: rows below (0), at (1) and above (2)
+// the node, read at columns c-1, c, c+1.
+template <typename T> struct Stencil {
+    const T *r0[3], *r1[3];
+    const uint8_t *m[3];
+    int c;
+};
+
+// Collide node (x, yc) from its populations f and the density stencil, then
+// push the post-collision populations: the reference sequence of
+// src/lbm.cpp:177-204 (repulsive force), :250-269 (equilibrium velocity),
+// src/fluid.cpp:254-276 + src/lbm.cpp:305-311 (equilibrium, BGK),
+// :333-337 (volume force), :404-427 (stream with half-way bounce-back).
+// Push one post-collision population: to the neighbour along c_i when it is a
+// fluid node, else back into the opposite direction at the node itself.
+template <typename S, typename T>
+__device__ __forceinline__ void push_one(const Fused2Args<S, T> &a, const int k, const int i,
+                                         const T v, const bool nf, const size_t node, const int x,
+                                         const int xl, const int xr, const int yc, const int yd,
+                                         const int yu)
+{
+    S *o = a.fout[k];
+    if (i == 0) {
+        Store<S>::st(o + node, v);
+    } else if (nf) {
+        const int xn = cx(i) == 0 ? x : (cx(i) > 0 ? xr : xl);
+        const int yn = cy(i) == 0 ? yc : (cy(i) > 0 ? yu : yd);
+        Store<S>::st(o + i * a.N + (size_t)yn * a.nx + xn, v);
+    } else {
+        Store<S>::st(o + opp(i) * a.N + node, v);
+    }
+}
+
+// f[k][i] gives population i of component k (registers or shared memory).
+template <typename S, typename T, typename Pops>
+__device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Pops &f,
+                                             const Stencil<T> &st, const int x, const int xl,
+                                             const int xr, const int yc, const int yd, const int yu)
+{
+    constexpr bool EXACT = sizeof(T) == 8;
+    const size_t N = a.N;
+    const int nx = a.nx;
+    const size_t node = (size_t)yc * nx + x;
+    if (!st.m[1][st.c]) {
+        // solid node: the reference's stream leaves zeros (src/lbm.cpp:431-434)
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+#pragma unroll
+            for (int i = 0; i < 9; ++i) Store<S>::st(a.fout[k] + i * N + node, T(0));
+    } else {
+        bool nf[9];
+        T p0[9], p1[9];
+#pragma unroll
+        for (int i = 1; i < 9; ++i) {
+            const int sl = cy(i) + 1;
+            const int col = st.c + cx(i);
+            nf[i] = st.m[sl][col] != 0;
+            p0[i] = st.r0[sl][col];
+            p1[i] = st.r1[sl][col];
+        }
+        const T psi0 = st.r0[1][st.c], psi1 = st.r1[1][st.c];
+        if constexpr (EXACT) {
+            // repulsive force, src/lbm.cpp:177-204
+            double F0x = 0.0, F0y = 0.0, F1x = 0.0, F1y = 0.0, Sx = 0.0, Sy = 0.0;
+#pragma unroll
+            for (int i = 1; i < 9; ++i) {
+                const double wcx = w_sc(i) * cx(i), wcy = w_sc(i) * cy(i);
+                if (nf[i]) {
+                    F0x += wcx * p1[i];
+                    F0y += wcy * p1[i];
+                    F1x += wcx * p0[i];
+                    F1y += wcy * p0[i];
+                } else {
+                    Sx += wcx; // solid sums, src/lbm.cpp:131-134
+                    Sy += wcy;
+                }
+            }
+            F0x *= a.c[0].gf * psi0;
+            F0y *= a.c[0].gf * psi0;
+            F1x *= a.c[1].gf * psi1;
+            F1y *= a.c[1].gf * psi1;
+            // momentum, src/lbm.cpp:250-255
+            double j0x = 0.0, j0y = 0.0, j1x = 0.0, j1y = 0.0;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                j0x += f[0][i] * double(cx(i));
+                j0y += f[0][i] * double(cy(i));
+                j1x += f[1][i] * double(cx(i));
+                j1y += f[1][i] * double(cy(i));
+            }
+            const double o0 = a.c[0].omega, o1 = a.c[1].omega;
+            const double ucx = (j0x * o0 + j1x * o1) / (psi0 * o0 + psi1 * o1);
+            const double ucy = (j0y * o0 + j1y * o1) / (psi0 * o0 + psi1 * o1);
+            const double psi[2] = {psi0, psi1};
+            const double Fx[2] = {F0x, F1x}, Fy[2] = {F0y, F1y};
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                double ux, uy;
+                if (!rho_is_zero(psi[k])) { // src/lbm.cpp:262-269
+                    double fsx, fsy;
+                    if (a.solid_from_mask) {
+                        fsx = a.c[k].gs_neg * Sx;
+                        fsy = a.c[k].gs_neg * Sy;
+                    } else {
+                        fsx = a.fsx[k][node];
+                        fsy = a.fsy[k][node];
+                    }
+                    const double io = a.c[k].inv_omega;
+                    ux = ucx + Fx[k] * io / psi[k] + fsx * io;
+                    uy = ucy + Fy[k] * io / psi[k] + fsy * io;
+                } else {
+                    ux = a.uex_old[k] ? a.uex_old[k][node] : 0.0;
+                    uy = a.uey_old[k] ? a.uey_old[k][node] : 0.0;
+                }
+                double fe[9];
+                feq_exact(psi[k], ux, uy, fe);
+                const double om = a.c[k].omega, omm = a.c[k].one_m_omega;
+#pragma unroll
+                for (int i = 0; i < 9; ++i) {
+                    double v = omm * f[k][i] + om * fe[i];
+                    if (a.c[k].force_on) v += a.c[k].force[i];
+                    push_one<S, T>(a, k, i, v, nf[i], node, x, xl, xr, yc, yd, yu);
+                }
+            }
+        } else {
+            // shifted form: the stencil holds rho - rho_ref
+            float A0x = 0.f, A0y = 0.f, A1x = 0.f, A1y = 0.f, Sx = 0.f, Sy = 0.f;
+#pragma unroll
+            for (int i = 1; i < 9; ++i) {
+                const float wcx = float(w_sc(i) * cx(i)), wcy = float(w_sc(i) * cy(i));
+                if (nf[i]) {
+                    if (cx(i)) { A0x = fmaf(wcx, p1[i], A0x); A1x = fmaf(wcx, p0[i], A1x); }
+                    if (cy(i)) { A0y = fmaf(wcy, p1[i], A0y); A1y = fmaf(wcy, p0[i], A1y); }
+                } else {
+                    Sx += wcx;
+                    Sy += wcy;
+                }
+            }
+            const float rr0 = a.c[0].rho_ref, rr1 = a.c[1].rho_ref;
+            const float r0 = rr0 + psi0, r1 = rr1 + psi1;
+            // sum over fluid neighbours of w c psi = A - rho_ref * S
+            const float F0x = a.c[0].gf * r0 * fmaf(-rr1, Sx, A0x);
+            const float F0y = a.c[0].gf * r0 * fmaf(-rr1, Sy, A0y);
+            const float F1x = a.c[1].gf * r1 * fmaf(-rr0, Sx, A1x);
+            const float F1y = a.c[1].gf * r1 * fmaf(-rr0, Sy, A1y);
+            float j0x = (f[0][1] - f[0][3]) + (f[0][5] - f[0][6]) + (f[0][8] - f[0][7]);
+            float j0y = (f[0][2] - f[0][4]) + (f[0][5] + f[0][6]) - (f[0][7] + f[0][8]);
+            float j1x = (f[1][1] - f[1][3]) + (f[1][5] - f[1][6]) + (f[1][8] - f[1][7]);
+            float j1y = (f[1][2] - f[1][4]) + (f[1][5] + f[1][6]) - (f[1][7] + f[1][8]);
+            const float o0 = a.c[0].omega, o1 = a.c[1].omega;
+            const float inv_den = 1.0f / fmaf(r0, o0, r1 * o1);
+            const float ucx = fmaf(j0x, o0, j1x * o1) * inv_den;
+            const float ucy = fmaf(j0y, o0, j1y * o1) * inv_den;
+            const float r[2] = {r0, r1}, dr[2] = {psi0, psi1};
+            const float Fx[2] = {F0x, F1x}, Fy[2] = {F0y, F1y};
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                float ux = ucx, uy = ucy;
+                if (!rho_is_zero(r[k])) {
+                    const float io = a.c[k].inv_omega;
+                    const float ir = io / r[k];
+                    ux = fmaf(Fx[k], ir, fmaf(a.c[k].gs_neg * Sx, io, ucx));
+                    uy = fmaf(Fy[k], ir, fmaf(a.c[k].gs_neg * Sy, io, ucy));
+                }
+                const float usq15 = 1.5f * fmaf(ux, ux, uy * uy);
+                const float om = a.c[k].omega;
+#pragma unroll
+                for (int i = 0; i < 9; ++i) {
+                    const float fe = feq_dev(i, dr[k], r[k], ux, uy, usq15);
+                    const T fi = f[k][i];
+                    float v = fmaf(om, fe - fi, fi);
+                    if (a.c[k].force_on) v += a.c[k].force[i];
+                    push_one<S, T>(a, k, i, v, nf[i], node, x, xl, xr, yc, yd, yu);
+                }
+            }
+        }
+    }
+}
+
+// shared-memory view of one node's populations in the ring: f[k][i]
+template <typename S, typename T, int P> struct RingPops {
+    const S *base; // stage base + column
+    struct Row {
+        const S *p;
+        __device__ __forceinline__ T operator[](int i) const { return T(p[i * P]); }
+    };
+    __device__ __forceinline__ Row operator[](int k) const { return Row{base + k * 9 * P}; }
+};
+
 // ---------------------------------------------------------------------------
 // kernel b: fused two-component step
 // ---------------------------------------------------------------------------
@@ -96,7 +285,6 @@ template <typename S, typename T, int TX, bool TWO_PASS>
 __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int xb, const int yb,
                                             T (&s_rho)[2][4][TX], uint8_t (&s_m)[4][TX])
 {
-    constexpr bool EXACT = sizeof(T) == 8;
     constexpr int W = TX - 2;
     const int t = threadIdx.x;
     const int nx = a.nx, ny = a.ny;
@@ -153,157 +341,10 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
             const int sc = r & 3, sm = (r - 1) & 3, sp = (r + 1) & 3;
             const int yc = wrap1(yb + r - 1, ny);
             const int yd = wrap1(yc - 1, ny), yu = wrap1(yc + 1, ny);
-            const size_t node = (size_t)yc * nx + x;
-            if (!s_m[sc][t]) {
-                // solid node: the reference's stream leaves zeros (src/lbm.cpp:431-434)
-#pragma unroll
-                for (int k = 0; k < 2; ++k)
-#pragma unroll
-                    for (int i = 0; i < 9; ++i) Store<S>::st(a.fout[k] + i * N + node, T(0));
-            } else {
-                bool nf[9];
-                T p0[9], p1[9];
-#pragma unroll
-                for (int i = 1; i < 9; ++i) {
-                    const int sl = cy(i) == 0 ? sc : (cy(i) > 0 ? sp : sm);
-                    const int col = t + cx(i);
-                    nf[i] = s_m[sl][col] != 0;
-                    p0[i] = s_rho[0][sl][col];
-                    p1[i] = s_rho[1][sl][col];
-                }
-                const T psi0 = s_rho[0][sc][t], psi1 = s_rho[1][sc][t];
-                T out[2][9];
-                if constexpr (EXACT) {
-                    // repulsive force, src/lbm.cpp:177-204
-                    double F0x = 0.0, F0y = 0.0, F1x = 0.0, F1y = 0.0, Sx = 0.0, Sy = 0.0;
-#pragma unroll
-                    for (int i = 1; i < 9; ++i) {
-                        const double wcx = w_sc(i) * cx(i), wcy = w_sc(i) * cy(i);
-                        if (nf[i]) {
-                            F0x += wcx * p1[i];
-                            F0y += wcy * p1[i];
-                            F1x += wcx * p0[i];
-                            F1y += wcy * p0[i];
-                        } else {
-                            Sx += wcx; // solid sums, src/lbm.cpp:131-134
-                            Sy += wcy;
-                        }
-                    }
-                    F0x *= a.c[0].gf * psi0;
-                    F0y *= a.c[0].gf * psi0;
-                    F1x *= a.c[1].gf * psi1;
-                    F1y *= a.c[1].gf * psi1;
-                    // momentum, src/lbm.cpp:250-255
-                    double j0x = 0.0, j0y = 0.0, j1x = 0.0, j1y = 0.0;
-#pragma unroll
-                    for (int i = 0; i < 9; ++i) {
-                        j0x += prev[0][i] * double(cx(i));
-                        j0y += prev[0][i] * double(cy(i));
-                        j1x += prev[1][i] * double(cx(i));
-                        j1y += prev[1][i] * double(cy(i));
-                    }
-                    const double o0 = a.c[0].omega, o1 = a.c[1].omega;
-                    const double ucx = (j0x * o0 + j1x * o1) / (psi0 * o0 + psi1 * o1);
-                    const double ucy = (j0y * o0 + j1y * o1) / (psi0 * o0 + psi1 * o1);
-                    const double psi[2] = {psi0, psi1};
-                    const double Fx[2] = {F0x, F1x}, Fy[2] = {F0y, F1y};
-#pragma unroll
-                    for (int k = 0; k < 2; ++k) {
-                        double ux, uy;
-                        if (!rho_is_zero(psi[k])) { // src/lbm.cpp:262-269
-                            double fsx, fsy;
-                            if (a.solid_from_mask) {
-                                fsx = a.c[k].gs_neg * Sx;
-                                fsy = a.c[k].gs_neg * Sy;
-                            } else {
-                                fsx = a.fsx[k][node];
-                                fsy = a.fsy[k][node];
-                            }
-                            const double io = a.c[k].inv_omega;
-                            ux = ucx + Fx[k] * io / psi[k] + fsx * io;
-                            uy = ucy + Fy[k] * io / psi[k] + fsy * io;
-                        } else {
-                            ux = a.uex_old[k] ? a.uex_old[k][node] : 0.0;
-                            uy = a.uey_old[k] ? a.uey_old[k][node] : 0.0;
-                        }
-                        double fe[9];
-                        feq_exact(psi[k], ux, uy, fe);
-                        const double om = a.c[k].omega, omm = a.c[k].one_m_omega;
-#pragma unroll
-                        for (int i = 0; i < 9; ++i) {
-                            double v = omm * prev[k][i] + om * fe[i];
-                            if (a.c[k].force_on) v += a.c[k].force[i];
-                            out[k][i] = v;
-                        }
-                    }
-                } else {
-                    // shifted form: s_rho holds rho - rho_ref
-                    float A0x = 0.f, A0y = 0.f, A1x = 0.f, A1y = 0.f, Sx = 0.f, Sy = 0.f;
-#pragma unroll
-                    for (int i = 1; i < 9; ++i) {
-                        const float wcx = float(w_sc(i) * cx(i)), wcy = float(w_sc(i) * cy(i));
-                        if (nf[i]) {
-                            if (cx(i)) { A0x = fmaf(wcx, p1[i], A0x); A1x = fmaf(wcx, p0[i], A1x); }
-                            if (cy(i)) { A0y = fmaf(wcy, p1[i], A0y); A1y = fmaf(wcy, p0[i], A1y); }
-                        } else {
-                            Sx += wcx;
-                            Sy += wcy;
-                        }
-                    }
-                    const float rr0 = a.c[0].rho_ref, rr1 = a.c[1].rho_ref;
-                    const float r0 = rr0 + psi0, r1 = rr1 + psi1;
-                    // sum over fluid neighbours of w c psi = A - rho_ref * S
-                    const float F0x = a.c[0].gf * r0 * fmaf(-rr1, Sx, A0x);
-                    const float F0y = a.c[0].gf * r0 * fmaf(-rr1, Sy, A0y);
-                    const float F1x = a.c[1].gf * r1 * fmaf(-rr0, Sx, A1x);
-                    const float F1y = a.c[1].gf * r1 * fmaf(-rr0, Sy, A1y);
-                    float j0x = (prev[0][1] - prev[0][3]) + (prev[0][5] - prev[0][6]) + (prev[0][8] - prev[0][7]);
-                    float j0y = (prev[0][2] - prev[0][4]) + (prev[0][5] + prev[0][6]) - (prev[0][7] + prev[0][8]);
-                    float j1x = (prev[1][1] - prev[1][3]) + (prev[1][5] - prev[1][6]) + (prev[1][8] - prev[1][7]);
-                    float j1y = (prev[1][2] - prev[1][4]) + (prev[1][5] + prev[1][6]) - (prev[1][7] + prev[1][8]);
-                    const float o0 = a.c[0].omega, o1 = a.c[1].omega;
-                    const float inv_den = 1.0f / fmaf(r0, o0, r1 * o1);
-                    const float ucx = fmaf(j0x, o0, j1x * o1) * inv_den;
-                    const float ucy = fmaf(j0y, o0, j1y * o1) * inv_den;
-                    const float r[2] = {r0, r1}, dr[2] = {psi0, psi1};
-                    const float Fx[2] = {F0x, F1x}, Fy[2] = {F0y, F1y};
-#pragma unroll
-                    for (int k = 0; k < 2; ++k) {
-                        float ux = ucx, uy = ucy;
-                        if (!rho_is_zero(r[k])) {
-                            const float io = a.c[k].inv_omega;
-                            const float ir = io / r[k];
-                            ux = fmaf(Fx[k], ir, fmaf(a.c[k].gs_neg * Sx, io, ucx));
-                            uy = fmaf(Fy[k], ir, fmaf(a.c[k].gs_neg * Sy, io, ucy));
-                        }
-                        const float usq15 = 1.5f * fmaf(ux, ux, uy * uy);
-                        const float om = a.c[k].omega;
-#pragma unroll
-                        for (int i = 0; i < 9; ++i) {
-                            const float fe = feq_dev(i, dr[k], r[k], ux, uy, usq15);
-                            float v = fmaf(om, fe - prev[k][i], prev[k][i]);
-                            if (a.c[k].force_on) v += a.c[k].force[i];
-                            out[k][i] = v;
-                        }
-                    }
-                }
-                // push streaming with half-way bounce-back, src/lbm.cpp:404-427
-#pragma unroll
-                for (int k = 0; k < 2; ++k) {
-                    S *o = a.fout[k];
-                    Store<S>::st(o + node, out[k][0]);
-#pragma unroll
-                    for (int i = 1; i < 9; ++i) {
-                        if (nf[i]) {
-                            const int xn = cx(i) == 0 ? x : (cx(i) > 0 ? xr : xl);
-                            const int yn = cy(i) == 0 ? yc : (cy(i) > 0 ? yu : yd);
-                            Store<S>::st(o + i * N + (size_t)yn * nx + xn, out[k][i]);
-                        } else {
-                            Store<S>::st(o + opp(i) * N + node, out[k][i]);
-                        }
-                    }
-                }
-            }
+            const Stencil<T> st{{s_rho[0][sm], s_rho[0][sc], s_rho[0][sp]},
+                                {s_rho[1][sm], s_rho[1][sc], s_rho[1][sp]},
+                                {s_m[sm], s_m[sc], s_m[sp]}, t};
+            collide_push<S, T>(a, prev, st, x, xl, xr, yc, yd, yu);
         }
 #pragma unroll
         for (int k = 0; k < 2; ++k)

@@ -404,3 +404,29 @@ cudaError_t launch_density_fp64(const uint8_t *mask, const double *f0, const dou
 }
 
 } // namespace sclbm
+
+// the FP64 batched kernel lives in this -fmad=false translation unit
+#include "batch_kernel.cuh"
+namespace sclbm {
+cudaError_t launch_batch_fp64(const Fused2Args<double, double> *doms, const TileRef *tiles,
+                              int ntiles, int parity, int grid, cudaStream_t s)
+{
+    return launch_batch_t<double, double>(doms, tiles, ntiles, parity, grid, s);
+}
+int batch_blocks_per_sm_fp64() { return batch_blocks_per_sm_t<double, double>(); }
+} // namespace sclbm
+
+// pipelined persistent FP64 kernels (-fmad=false keeps them bit-exact)
+#include "fused_async.cuh"
+namespace sclbm {
+cudaError_t launch_fused2_async_fp64(const Fused2Args<double, double> &a, cudaStream_t s)
+{
+    return launch_fused2_async_t<double, double, 128, 3>(a, s);
+}
+cudaError_t launch_batch2_async_fp64(const Fused2Args<double, double> *doms,
+                                     const long long *prefix, int ndom, long long units,
+                                     int parity, cudaStream_t s)
+{
+    return launch_batch2_async_t<double, double, 128, 3>(doms, prefix, ndom, units, parity, s);
+}
+} // namespace sclbm

@@ -40,3 +40,39 @@ cudaError_t launch_density_f16(const uint8_t *mask, const __half *f0, const __ha
 }
 
 } // namespace sclbm
+
+#include "batch_kernel.cuh"
+namespace sclbm {
+cudaError_t launch_batch_f32(const Fused2Args<float, float> *doms, const TileRef *tiles,
+                             int ntiles, int parity, int grid, cudaStream_t s)
+{
+    return launch_batch_t<float, float>(doms, tiles, ntiles, parity, grid, s);
+}
+cudaError_t launch_batch_f16(const Fused2Args<__half, float> *doms, const TileRef *tiles,
+                             int ntiles, int parity, int grid, cudaStream_t s)
+{
+    return launch_batch_t<__half, float>(doms, tiles, ntiles, parity, grid, s);
+}
+int batch_blocks_per_sm_fp64();
+int batch_blocks_per_sm(sclbm_precision p)
+{
+    switch (p) {
+    case SCLBM_FP64: return batch_blocks_per_sm_fp64();
+    case SCLBM_FP32_SHIFTED: return batch_blocks_per_sm_t<float, float>();
+    default: return batch_blocks_per_sm_t<__half, float>();
+    }
+}
+} // namespace sclbm
+
+#include "fused_async.cuh"
+namespace sclbm {
+cudaError_t launch_fused2_async_f32(const Fused2Args<float, float> &a, cudaStream_t s)
+{
+    return launch_fused2_async_t<float, float, 128, 4>(a, s);
+}
+cudaError_t launch_batch2_async_f32(const Fused2Args<float, float> *doms, const long long *prefix,
+                                    int ndom, long long units, int parity, cudaStream_t s)
+{
+    return launch_batch2_async_t<float, float, 128, 4>(doms, prefix, ndom, units, parity, s);
+}
+} // namespace sclbm

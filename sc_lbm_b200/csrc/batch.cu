@@ -3,10 +3,11 @@
 // CUDA graph and replayed.  All domains of a batch share the storage precision
 // and the buffer parity.  Two work decompositions:
 //
-//  * units (default for FP64/FP32): the rows of the 128-column strips of all
-//    domains are concatenated and cut into equal contiguous chunks, one per
-//    resident CTA (fused_async.cuh); balanced to a row whatever the domain
-//    sizes;
+//  * bands (default for FP64/FP32): every domain is cut into 128-column strips
+//    and row bands of one common height, chosen as the smallest for which all
+//    (domain, strip, band) tiles are resident at once; neighbouring strips of
+//    a band are adjacent in the list so they walk the same rows together; the
+//    pipelined single-pass body (fused_async.cuh) runs each tile;
 //  * tile list (FP16, or on request): every tile (126 columns x tile_y rows)
 //    of every domain, largest first; CTA b takes tiles b, b+grid, ... and runs
 //    the register-tile body (batch_kernel.cuh).
@@ -15,6 +16,7 @@
 
 #include "domain.h"
 #include "batch_kernel.cuh"
+#include "fused_async.cuh"
 
 
 using namespace sclbm;
@@ -26,8 +28,8 @@ struct sclbm_batch {
     sclbm_precision prec = SCLBM_FP32_SHIFTED;
     void *d_args = nullptr;  // Fused2Args<S,T>[2*ndom] (parity 0, parity 1)
     TileRef *d_tiles = nullptr;
-    long long *d_prefix = nullptr; // first unit of each domain, then the total
-    long long units = 0;
+    BandTile *d_bands = nullptr; // (domain, strip, band) tiles of the pipelined kernel
+    int nbands = 0, band_grid = 0, band_rows = 0;
     int ntiles = 0, grid = 0, parity = 0;
     int use_units = 1;
     cudaGraphExec_t graph[2] = {nullptr, nullptr}; // by starting parity
@@ -36,13 +38,12 @@ struct sclbm_batch {
 
 static cudaError_t batch_launch_any(sclbm_batch *b, int parity, cudaStream_t s)
 {
-    const int nd = (int)b->doms.size();
     if (b->use_units && b->prec == SCLBM_FP64)
-        return launch_batch2_async_fp64((const Fused2Args<double, double> *)b->d_args, b->d_prefix,
-                                        nd, b->units, parity, s);
+        return launch_batch2_async_fp64((const Fused2Args<double, double> *)b->d_args, b->d_bands,
+                                        b->nbands, b->band_grid, parity, s);
     if (b->use_units && b->prec == SCLBM_FP32_SHIFTED)
-        return launch_batch2_async_f32((const Fused2Args<float, float> *)b->d_args, b->d_prefix,
-                                       nd, b->units, parity, s);
+        return launch_batch2_async_f32((const Fused2Args<float, float> *)b->d_args, b->d_bands,
+                                       b->nbands, b->band_grid, parity, s);
     switch (b->prec) {
     case SCLBM_FP64:
         return launch_batch_fp64((const Fused2Args<double, double> *)b->d_args, b->d_tiles,
@@ -92,7 +93,7 @@ void sclbm_batch_destroy(sclbm_batch *b)
         if (g) cudaGraphExecDestroy(g);
     if (b->d_args) cudaFree(b->d_args);
     if (b->d_tiles) cudaFree(b->d_tiles);
-    if (b->d_prefix) cudaFree(b->d_prefix);
+    if (b->d_bands) cudaFree(b->d_bands);
     delete b;
 }
 
@@ -140,18 +141,39 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
     case SCLBM_FP32_SHIFTED: rc = upload_args<float, float>(b, ty); break;
     default: rc = upload_args<__half, float>(b, ty); break;
     }
-    std::vector<long long> prefix(ndomains + 1, 0);
-    for (int k = 0; k < ndomains; ++k) {
-        const sclbm_domain *d = b->doms[k];
-        prefix[k + 1] = prefix[k] + (long long)((d->nx + ASYNC_STRIP - 1) / ASYNC_STRIP) * d->ny;
-    }
-    b->units = prefix[ndomains];
+    // pipelined kernel: the smallest band height whose (domain, strip, band)
+    // tiles all fit resident at once, bands of one domain split its rows evenly
     b->use_units = b->prec != SCLBM_FP16_SHIFTED;
-    if (!rc && cudaMalloc(&b->d_prefix, prefix.size() * sizeof(long long)) != cudaSuccess)
-        rc = set_error(SCLBM_E_CUDA, "unit prefix allocation");
-    if (!rc && cudaMemcpy(b->d_prefix, prefix.data(), prefix.size() * sizeof(long long),
-                          cudaMemcpyHostToDevice) != cudaSuccess)
-        rc = set_error(SCLBM_E_CUDA, "unit prefix upload");
+    std::vector<BandTile> bands;
+    if (b->use_units) {
+        const int res = std::max(1, b->prec == SCLBM_FP64 ? async_resident_fp64() : async_resident_f32());
+        int H = 4;
+        auto count = [&](int h) {
+            long long n = 0;
+            for (auto *d : b->doms)
+                n += (long long)((d->nx + ASYNC_STRIP - 1) / ASYNC_STRIP) * ((d->ny + h - 1) / h);
+            return n;
+        };
+        int max_ny = 1;
+        for (auto *d : b->doms) max_ny = std::max(max_ny, (int)d->ny);
+        while (count(H) > res && H < max_ny) ++H;
+        b->band_rows = H;
+        for (int k = 0; k < ndomains; ++k) {
+            const sclbm_domain *d = b->doms[k];
+            const int nb = (int)((d->ny + H - 1) / H), ns = (int)((d->nx + ASYNC_STRIP - 1) / ASYNC_STRIP);
+            for (int j = 0; j < nb; ++j) {
+                const int y0 = (int)((long long)d->ny * j / nb), y1 = (int)((long long)d->ny * (j + 1) / nb);
+                for (int s = 0; s < ns; ++s) bands.push_back(BandTile{k, s * ASYNC_STRIP, y0, y1});
+            }
+        }
+        b->nbands = (int)bands.size();
+        b->band_grid = std::max(1, std::min(b->nbands, res));
+        if (!rc && cudaMalloc(&b->d_bands, bands.size() * sizeof(BandTile)) != cudaSuccess)
+            rc = set_error(SCLBM_E_CUDA, "band list allocation");
+        if (!rc && cudaMemcpy(b->d_bands, bands.data(), bands.size() * sizeof(BandTile),
+                              cudaMemcpyHostToDevice) != cudaSuccess)
+            rc = set_error(SCLBM_E_CUDA, "band list upload");
+    }
     if (!rc && cudaMalloc(&b->d_tiles, sorted.size() * sizeof(TileRef)) != cudaSuccess)
         rc = set_error(SCLBM_E_CUDA, "tile list allocation");
     if (!rc && cudaMemcpy(b->d_tiles, sorted.data(), sorted.size() * sizeof(TileRef),

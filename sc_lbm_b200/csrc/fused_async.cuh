@@ -144,46 +144,37 @@ __device__ __forceinline__ void async_segment(const Fused2Args<S, T> &a, const i
     __syncthreads(); // the rings are reused by the next segment
 }
 
+// Grid (strips, bands): CTA (s, b) owns strip s, rows [b*ny/B, (b+1)*ny/B).
+// The bands split every strip at the same rows and neighbouring strips have
+// consecutive CTA indices, so the CTAs of one band walk the same rows at the
+// same time: a strip's halo columns and the sectors its pushes share with the
+// next strip are touched by both within a few rows (L2 hits, whole-sector
+// writes).
 template <typename S, typename T, int TX, int R>
 __global__ void __launch_bounds__(TX) k_fused2_async(const __grid_constant__ Fused2Args<S, T> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    const int nstrips = (a.nx + TX - 1) / TX;
-    const long long U = (long long)nstrips * a.ny;
-    const long long u0 = U * blockIdx.x / gridDim.x, u1 = U * (blockIdx.x + 1) / gridDim.x;
-    for (long long u = u0; u < u1;) {
-        const int s = int(u / a.ny), y0 = int(u % a.ny);
-        const int y1 = (int)min((long long)a.ny, (long long)y0 + (u1 - u));
-        async_segment<S, T, TX, R>(a, s * TX, y0, y1, smem);
-        u += y1 - y0;
-    }
+    const int y0 = (int)((long long)a.ny * blockIdx.y / gridDim.y);
+    const int y1 = (int)((long long)a.ny * (blockIdx.y + 1) / gridDim.y);
+    if (y1 > y0) async_segment<S, T, TX, R>(a, blockIdx.x * TX, y0, y1, smem);
 }
 
-// Batched form: the units of all domains are concatenated (prefix[d] = first
-// unit of domain d, prefix[ndom] = total) and split the same way.
+// Batched form: a list of (domain, strip, row band) tiles, neighbouring strips
+// of a band adjacent in the list; CTA i takes tiles i, i + grid, ...
+struct BandTile {
+    int dom, xb, y0, y1;
+};
+
 template <typename S, typename T, int TX, int R>
 __global__ void __launch_bounds__(TX)
-    k_batch2_async(const Fused2Args<S, T> *__restrict__ doms, const long long *__restrict__ prefix,
-                   int ndom, int parity)
+    k_batch2_async(const Fused2Args<S, T> *__restrict__ doms, const BandTile *__restrict__ tiles,
+                   int ntiles, int parity)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    const long long U = prefix[ndom];
-    const long long u0 = U * blockIdx.x / gridDim.x, u1 = U * (blockIdx.x + 1) / gridDim.x;
-    int lo = 0, hi = ndom - 1; // last domain with prefix[d] <= u0
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (prefix[mid] <= u0) lo = mid;
-        else hi = mid - 1;
-    }
-    int d = lo;
-    for (long long u = u0; u < u1;) {
-        while (prefix[d + 1] <= u) ++d;
-        const Fused2Args<S, T> a = doms[2 * d + parity];
-        const long long local = u - prefix[d];
-        const int s = int(local / a.ny), y0 = int(local % a.ny);
-        const int y1 = (int)min((long long)a.ny, (long long)y0 + (u1 - u));
-        async_segment<S, T, TX, R>(a, s * TX, y0, y1, smem);
-        u += y1 - y0;
+    for (int i = blockIdx.x; i < ntiles; i += gridDim.x) {
+        const BandTile tl = tiles[i];
+        const Fused2Args<S, T> a = doms[2 * tl.dom + parity];
+        async_segment<S, T, TX, R>(a, tl.xb, tl.y0, tl.y1, smem);
     }
 }
 
@@ -206,23 +197,28 @@ inline cudaError_t launch_fused2_async_t(const Fused2Args<S, T> &a, cudaStream_t
     using L = AsyncLayout<S, T, TX, R>;
     static int per_sm = resident_ctas(k_fused2_async<S, T, TX, R>, TX, L::bytes);
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    const long long U = (long long)((a.nx + TX - 1) / TX) * a.ny;
-    long long grid = (long long)per_sm * sm_count();
-    grid = std::max(1LL, std::min(grid, U / 4));
-    k_fused2_async<S, T, TX, R><<<(int)grid, TX, L::bytes, s>>>(a);
+    const int nstrips = (a.nx + TX - 1) / TX;
+    // as many bands as fit resident beside each other, at least 4 rows each
+    int nbands = std::max(1, per_sm * sm_count() / nstrips);
+    nbands = std::max(1, std::min(nbands, a.ny / 4));
+    k_fused2_async<S, T, TX, R><<<dim3(nstrips, nbands), TX, L::bytes, s>>>(a);
     return cudaGetLastError();
 }
 
-template <typename S, typename T, int TX, int R>
-inline cudaError_t launch_batch2_async_t(const Fused2Args<S, T> *doms, const long long *prefix,
-                                         int ndom, long long units, int parity, cudaStream_t s)
+template <typename S, typename T, int TX, int R> inline int async_resident_ctas()
 {
     using L = AsyncLayout<S, T, TX, R>;
     static int per_sm = resident_ctas(k_batch2_async<S, T, TX, R>, TX, L::bytes);
-    if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    long long grid = (long long)per_sm * sm_count();
-    grid = std::max(1LL, std::min(grid, units / 4));
-    k_batch2_async<S, T, TX, R><<<(int)grid, TX, L::bytes, s>>>(doms, prefix, ndom, parity);
+    return per_sm * sm_count();
+}
+
+template <typename S, typename T, int TX, int R>
+inline cudaError_t launch_batch2_async_t(const Fused2Args<S, T> *doms, const BandTile *tiles,
+                                         int ntiles, int grid, int parity, cudaStream_t s)
+{
+    using L = AsyncLayout<S, T, TX, R>;
+    if (async_resident_ctas<S, T, TX, R>() < 1) return cudaErrorInvalidConfiguration;
+    k_batch2_async<S, T, TX, R><<<grid, TX, L::bytes, s>>>(doms, tiles, ntiles, parity);
     return cudaGetLastError();
 }
 

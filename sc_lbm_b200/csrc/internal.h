@@ -112,15 +112,17 @@ cudaError_t launch_fused1_f32(const Fused1Args<float, float> &a, cudaStream_t s)
 cudaError_t launch_fused2_f16(const Fused2Args<__half, float> &a, int variant, int tx,
                               cudaStream_t s);
 cudaError_t launch_fused1_f16(const Fused1Args<__half, float> &a, cudaStream_t s);
-// pipelined persistent single-pass kernels (fused_async.cuh); units of the
-// batched form are strips(128 columns) x rows, prefix[] their running sums
+// pipelined single-pass kernels (fused_async.cuh): 128-column strips cut into
+// row bands; the batched form walks a list of (domain, strip, band) tiles
+struct BandTile;
 cudaError_t launch_fused2_async_fp64(const Fused2Args<double, double> &a, cudaStream_t s);
 cudaError_t launch_fused2_async_f32(const Fused2Args<float, float> &a, cudaStream_t s);
-cudaError_t launch_batch2_async_fp64(const Fused2Args<double, double> *doms,
-                                     const long long *prefix, int ndom, long long units,
-                                     int parity, cudaStream_t s);
-cudaError_t launch_batch2_async_f32(const Fused2Args<float, float> *doms, const long long *prefix,
-                                    int ndom, long long units, int parity, cudaStream_t s);
+cudaError_t launch_batch2_async_fp64(const Fused2Args<double, double> *doms, const BandTile *tiles,
+                                     int ntiles, int grid, int parity, cudaStream_t s);
+cudaError_t launch_batch2_async_f32(const Fused2Args<float, float> *doms, const BandTile *tiles,
+                                    int ntiles, int grid, int parity, cudaStream_t s);
+int async_resident_fp64(); // CTAs of the batched kernel resident on the device
+int async_resident_f32();
 constexpr int ASYNC_STRIP = 128;
 // density pass (kernel a): rho (or rho - rho_ref for shifted storage) per node,
 // 0 at solid nodes; both components in one launch

@@ -423,10 +423,10 @@ cudaError_t launch_fused2_async_fp64(const Fused2Args<double, double> &a, cudaSt
 {
     return launch_fused2_async_t<double, double, 128, 3>(a, s);
 }
-cudaError_t launch_batch2_async_fp64(const Fused2Args<double, double> *doms,
-                                     const long long *prefix, int ndom, long long units,
-                                     int parity, cudaStream_t s)
+cudaError_t launch_batch2_async_fp64(const Fused2Args<double, double> *doms, const BandTile *tiles,
+                                     int ntiles, int grid, int parity, cudaStream_t s)
 {
-    return launch_batch2_async_t<double, double, 128, 3>(doms, prefix, ndom, units, parity, s);
+    return launch_batch2_async_t<double, double, 128, 3>(doms, tiles, ntiles, grid, parity, s);
 }
+int async_resident_fp64() { return async_resident_ctas<double, double, 128, 3>(); }
 } // namespace sclbm

@@ -70,9 +70,10 @@ cudaError_t launch_fused2_async_f32(const Fused2Args<float, float> &a, cudaStrea
 {
     return launch_fused2_async_t<float, float, 128, 4>(a, s);
 }
-cudaError_t launch_batch2_async_f32(const Fused2Args<float, float> *doms, const long long *prefix,
-                                    int ndom, long long units, int parity, cudaStream_t s)
+cudaError_t launch_batch2_async_f32(const Fused2Args<float, float> *doms, const BandTile *tiles,
+                                    int ntiles, int grid, int parity, cudaStream_t s)
 {
-    return launch_batch2_async_t<float, float, 128, 4>(doms, prefix, ndom, units, parity, s);
+    return launch_batch2_async_t<float, float, 128, 4>(doms, tiles, ntiles, grid, parity, s);
 }
+int async_resident_f32() { return async_resident_ctas<float, float, 128, 4>(); }
 } // namespace sclbm

@@ -240,7 +240,7 @@ int sclbm_domain_mass_momentum(sclbm_domain *d, double out[7]);
  *   2 = single pass, one tile per CTA, rows held in registers.
  * tile_y = rows per tile of variants 1 and 2 (0 keeps the default). */
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y);
-/* Threads per tile of the two-component kernel: 64, 128 (default) or 256. */
+/* Threads per tile of the register-tile kernel (variants 1, 2): 64 or 128. */
 int sclbm_domain_set_threads(sclbm_domain *d, int tx);
 /* Device bytes held by the domain. */
 size_t sclbm_domain_device_bytes(const sclbm_domain *d);

@@ -25,7 +25,7 @@ __global__ void __launch_bounds__(BATCH_TX)
     for (int i = blockIdx.x; i < ntiles; i += gridDim.x) {
         const TileRef tr = tiles[i];
         const Fused2Args<S, T> a = doms[2 * tr.dom + parity];
-        fused2_tile<S, T, BATCH_TX, false>(a, tr.xb, tr.yb, s_rho, s_m);
+        fused2_tile<S, T, BATCH_TX, false, KF_FORCE | KF_SOLID>(a, tr.xb, tr.yb, s_rho, s_m);
         __syncthreads(); // the shared ring is reused by the next tile
     }
 }

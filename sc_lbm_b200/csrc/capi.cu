@@ -101,6 +101,7 @@ int geometry_device_mask(const sclbm_geometry *g, const uint8_t **out)
         SCLBM_CUDA(cudaMemcpyAsync(g->d_mask, h.data(), N, cudaMemcpyHostToDevice, stream()));
         SCLBM_CUDA(cudaStreamSynchronize(stream()));
         g->dirty = false;
+        g->has_solid = std::find(h.begin(), h.end(), (uint8_t)0) != h.end();
     }
     *out = g->d_mask;
     return SCLBM_OK;
@@ -693,6 +694,7 @@ int sclbm_lbm_step(sclbm_lbm *l, const sclbm_geometry *g, sclbm_fluid *f1, sclbm
         a.uey_old[k] = fl[k]->d[SCLBM_FIELD_UEQ_Y];
     }
     a.solid_from_mask = 0;
+    a.has_solid = g->has_solid ? 1 : 0;
     for (int s = 0; s < nsteps; ++s) {
         a.fin[0] = f1->d[SCLBM_FIELD_F];
         a.fin[1] = f2->d[SCLBM_FIELD_F];

@@ -210,6 +210,7 @@ static void fill2(const sclbm_domain *d, Fused2Args<S, T> &a)
         fill_comp<T>(a.c[k], d->p, k);
     }
     a.solid_from_mask = 1;
+    a.has_solid = d->has_solid ? 1 : 0;
 }
 
 void domain_fused2_args(const sclbm_domain *d, Fused2Args<double, double> *a64,
@@ -333,6 +334,7 @@ int sclbm_domain_create(size_t nx, size_t ny, const int32_t *mask, const sclbm_p
     d->N = N;
     d->ncomp = p->ncomp;
     d->prec = precision;
+    d->has_solid = std::find(hm.begin(), hm.end(), (uint8_t)0) != hm.end();
     d->p = *p;
     if (precision == SCLBM_FP64) d->p.rho_ref[0] = d->p.rho_ref[1] = 0.0;
     const size_t es = elem_size(precision);
@@ -382,8 +384,8 @@ int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y)
 int sclbm_domain_set_threads(sclbm_domain *d, int tx)
 {
     if (!d) return set_error(SCLBM_E_INVALID_ARGUMENT, "null domain");
-    if (tx != 64 && tx != 128 && tx != 256)
-        return set_error(SCLBM_E_INVALID_ARGUMENT, "threads per tile must be 64, 128 or 256");
+    if (tx != 64 && tx != 128)
+        return set_error(SCLBM_E_INVALID_ARGUMENT, "threads per tile must be 64 or 128");
     d->tx = tx;
     return SCLBM_OK;
 }

@@ -17,6 +17,7 @@ struct sclbm_domain {
     int variant = 0;  // 0 single pass, 1 two pass
     int tile_y = 0;   // rows per tile (0: default)
     int tx = 128;     // threads per CTA
+    bool has_solid = true; // the mask has solid nodes
     size_t bytes = 0; // device bytes held
 };
 

@@ -1,24 +1,25 @@
-// fused_async.cuh -- persistent, load-balanced variant of the fused step with
-// the population rows staged through a shared-memory ring by asynchronous
-// global->shared copies (cp.async / LDGSTS).
+// fused_async.cuh -- variant of the fused step whose population rows are
+// staged through a shared-memory ring by asynchronous global->shared copies
+// (cp.async / LDGSTS), with a band decomposition of the lattice.
 //
 // Work decomposition.  The lattice is cut into column strips of TX columns
-// (one thread per column, all threads interior); a "unit" is one row of one
-// strip.  The U = strips x ny units are split into gridDim.x contiguous,
-// equal chunks, one per CTA, and the grid is sized to the number of CTAs
-// that are resident at once, so every SM finishes together (no tail wave).
-// A chunk is processed as one or more segments (a run of rows inside one
-// strip); each segment reads two halo rows and two halo columns.
+// (one thread per column, all threads interior) and row bands; CTA (s, b)
+// owns strip s, band b.  The bands split every strip at the same rows and
+// neighbouring strips have consecutive CTA indices, so the CTAs of one band
+// walk the same rows at the same time: a strip's halo columns and the sectors
+// its pushes share with the next strip are touched by both within a few rows
+// (L2 hits, whole-sector writes).  The number of bands is chosen so that all
+// CTAs are resident at once.
 //
-// Pipeline.  For a segment, local row lr (0 = the halo row below, nrow+1 =
-// the halo row above) lives in ring stage lr % R.  Before the row loop, rows
-// 0..R-2 are requested; iteration lr waits for row lr, reduces it to the
-// densities of both components (shared density ring, one __syncthreads),
-// collides row lr-1 from its populations still in the ring, pushes the
-// results to global memory, and finally requests row lr+R-1 into the stage
-// that row lr-1 just vacated.  Each thread copies and reads only its own
-// column (threads 0 and ncol-1 also the halo columns), so the population ring
-// needs no barrier; R-1 rows per thread are in flight while it computes.
+// Pipeline.  For a segment of rows [y0, y1), local row lr (0 = the halo row
+// below, nrow+1 = the halo row above) lives in ring stage lr % R.  Before the
+// row loop, rows 0..R-2 are requested; iteration lr waits for row lr, reduces
+// it to the densities of both components (shared density ring, one
+// __syncthreads), collides row lr-1 from its populations still in the ring,
+// pushes the results to global memory, and finally requests row lr+R-1 into
+// the stage that row lr-1 just vacated.  Each thread copies and reads only its
+// own column (threads 0 and ncol-1 also the halo columns), so the population
+// ring needs no barrier; R-1 rows per thread are in flight while it computes.
 #pragma once
 #include <cuda_pipeline.h>
 
@@ -35,7 +36,7 @@ template <typename S, typename T, int TX, int R> struct AsyncLayout {
 
 template <typename S, typename T, int TX, int R>
 __device__ __forceinline__ void async_copy_node(S *pops, int stage, int col,
-                                                const Fused2Args<S, T> &a, size_t node)
+                                                const Fused2Args<S, T> &a, uint32_t node)
 {
     constexpr int P = TX + 2;
 #pragma unroll
@@ -43,7 +44,7 @@ __device__ __forceinline__ void async_copy_node(S *pops, int stage, int col,
 #pragma unroll
         for (int i = 0; i < 9; ++i)
             __pipeline_memcpy_async(pops + ((stage * 2 + k) * 9 + i) * P + col,
-                                    a.fin[k] + i * a.N + node, sizeof(S));
+                                    a.fin[k] + (size_t)i * a.N + node, sizeof(S));
 }
 
 template <typename S, typename T, int TX, int R>
@@ -65,12 +66,13 @@ __device__ __forceinline__ void async_density(const S *pops, int stage, int col,
 }
 
 // Rows [y0, y1) of the strip starting at column xb.
-template <typename S, typename T, int TX, int R>
+template <typename S, typename T, int TX, int R, int FLAGS>
 __device__ __forceinline__ void async_segment(const Fused2Args<S, T> &a, const int xb,
                                               const int y0, const int y1, unsigned char *smem)
 {
     using L = AsyncLayout<S, T, TX, R>;
     constexpr int P = L::P;
+    constexpr bool SOLID = (FLAGS & KF_SOLID) != 0;
     S *pops = reinterpret_cast<S *>(smem);
     T *rho = reinterpret_cast<T *>(smem + L::pops);
     uint8_t *msk = smem + L::pops + L::rho;
@@ -89,7 +91,7 @@ __device__ __forceinline__ void async_segment(const Fused2Args<S, T> &a, const i
     int issue_stage = 0;
     auto issue = [&](int lr) {
         if (act && lr <= last) {
-            const size_t row = (size_t)wrap1(y0 - 1 + lr, ny) * nx;
+            const uint32_t row = (uint32_t)wrap1(y0 - 1 + lr, ny) * (uint32_t)nx;
             async_copy_node<S, T, TX, R>(pops, issue_stage, t + 1, a, row + x);
             if (hl) async_copy_node<S, T, TX, R>(pops, issue_stage, 0, a, row + xhl);
             if (hr) async_copy_node<S, T, TX, R>(pops, issue_stage, ncol + 1, a, row + xhr);
@@ -100,20 +102,20 @@ __device__ __forceinline__ void async_segment(const Fused2Args<S, T> &a, const i
 #pragma unroll
     for (int q = 0; q < R - 1; ++q) issue(q);
 
-    uint8_t mn = 0, mnl = 0, mnr = 0; // masks of the next row (loaded one row ahead)
-    if (act) {
-        const size_t row = (size_t)wrap1(y0 - 1, ny) * nx;
+    uint8_t mn = 1, mnl = 1, mnr = 1; // masks of the next row (loaded one row ahead)
+    if (SOLID && act) {
+        const uint32_t row = (uint32_t)wrap1(y0 - 1, ny) * (uint32_t)nx;
         mn = a.mask[row + x];
         if (hl) mnl = a.mask[row + xhl];
         if (hr) mnr = a.mask[row + xhr];
     }
-    int stage = 0;                     // ring stage of row lr
-    int cstage = R - 1;                // ring stage of row lr-1
+    int stage = 0;      // ring stage of row lr
+    int cstage = R - 1; // ring stage of row lr-1
     for (int lr = 0; lr <= last; ++lr) {
         const int slot = lr & 3;
         const uint8_t m = mn, ml = mnl, mr = mnr;
-        if (act && lr < last) {
-            const size_t row = (size_t)wrap1(y0 + lr, ny) * nx;
+        if (SOLID && act && lr < last) {
+            const uint32_t row = (uint32_t)wrap1(y0 + lr, ny) * (uint32_t)nx;
             mn = a.mask[row + x];
             if (hl) mnl = a.mask[row + xhl];
             if (hr) mnr = a.mask[row + xhr];
@@ -127,13 +129,13 @@ __device__ __forceinline__ void async_segment(const Fused2Args<S, T> &a, const i
         __syncthreads();
         if (act && lr >= 2) {
             const int yc = wrap1(y0 + lr - 2, ny);
-            const int yd = wrap1(yc - 1, ny), yu = wrap1(yc + 1, ny);
             const int sm = (lr - 2) & 3, sc = (lr - 1) & 3, sp = slot;
             const RingPops<S, T, P> f{pops + cstage * 18 * P + t + 1};
             const Stencil<T> st{{rho + (0 * 4 + sm) * P, rho + (0 * 4 + sc) * P, rho + (0 * 4 + sp) * P},
                                 {rho + (1 * 4 + sm) * P, rho + (1 * 4 + sc) * P, rho + (1 * 4 + sp) * P},
                                 {msk + sm * P, msk + sc * P, msk + sp * P}, t + 1};
-            collide_push<S, T>(a, f, st, x, xl, xr, yc, yd, yu);
+            const Nbr n = make_nbr(nx, x, xl, xr, yc, wrap1(yc - 1, ny), wrap1(yc + 1, ny));
+            collide_push<S, T, FLAGS>(a, f, st, n);
         }
         // row lr-1's stage is free again: request row lr+R-1 into it
         issue(lr + R - 1);
@@ -145,18 +147,13 @@ __device__ __forceinline__ void async_segment(const Fused2Args<S, T> &a, const i
 }
 
 // Grid (strips, bands): CTA (s, b) owns strip s, rows [b*ny/B, (b+1)*ny/B).
-// The bands split every strip at the same rows and neighbouring strips have
-// consecutive CTA indices, so the CTAs of one band walk the same rows at the
-// same time: a strip's halo columns and the sectors its pushes share with the
-// next strip are touched by both within a few rows (L2 hits, whole-sector
-// writes).
-template <typename S, typename T, int TX, int R>
+template <typename S, typename T, int TX, int R, int FLAGS>
 __global__ void __launch_bounds__(TX) k_fused2_async(const __grid_constant__ Fused2Args<S, T> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int y0 = (int)((long long)a.ny * blockIdx.y / gridDim.y);
     const int y1 = (int)((long long)a.ny * (blockIdx.y + 1) / gridDim.y);
-    if (y1 > y0) async_segment<S, T, TX, R>(a, blockIdx.x * TX, y0, y1, smem);
+    if (y1 > y0) async_segment<S, T, TX, R, FLAGS>(a, blockIdx.x * TX, y0, y1, smem);
 }
 
 // Batched form: a list of (domain, strip, row band) tiles, neighbouring strips
@@ -165,7 +162,7 @@ struct BandTile {
     int dom, xb, y0, y1;
 };
 
-template <typename S, typename T, int TX, int R>
+template <typename S, typename T, int TX, int R, int FLAGS>
 __global__ void __launch_bounds__(TX)
     k_batch2_async(const Fused2Args<S, T> *__restrict__ doms, const BandTile *__restrict__ tiles,
                    int ntiles, int parity)
@@ -174,7 +171,7 @@ __global__ void __launch_bounds__(TX)
     for (int i = blockIdx.x; i < ntiles; i += gridDim.x) {
         const BandTile tl = tiles[i];
         const Fused2Args<S, T> a = doms[2 * tl.dom + parity];
-        async_segment<S, T, TX, R>(a, tl.xb, tl.y0, tl.y1, smem);
+        async_segment<S, T, TX, R, FLAGS>(a, tl.xb, tl.y0, tl.y1, smem);
     }
 }
 
@@ -191,24 +188,37 @@ template <typename K> inline int resident_ctas(K kernel, int threads, size_t sme
     return n;
 }
 
-template <typename S, typename T, int TX, int R>
-inline cudaError_t launch_fused2_async_t(const Fused2Args<S, T> &a, cudaStream_t s)
+template <typename S, typename T, int TX, int R, int FLAGS>
+inline cudaError_t launch_fused2_async_f(const Fused2Args<S, T> &a, cudaStream_t s)
 {
     using L = AsyncLayout<S, T, TX, R>;
-    static int per_sm = resident_ctas(k_fused2_async<S, T, TX, R>, TX, L::bytes);
+    static int per_sm = resident_ctas(k_fused2_async<S, T, TX, R, FLAGS>, TX, L::bytes);
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     const int nstrips = (a.nx + TX - 1) / TX;
     // as many bands as fit resident beside each other, at least 4 rows each
     int nbands = std::max(1, per_sm * sm_count() / nstrips);
     nbands = std::max(1, std::min(nbands, a.ny / 4));
-    k_fused2_async<S, T, TX, R><<<dim3(nstrips, nbands), TX, L::bytes, s>>>(a);
+    k_fused2_async<S, T, TX, R, FLAGS><<<dim3(nstrips, nbands), TX, L::bytes, s>>>(a);
     return cudaGetLastError();
 }
 
+template <typename S, typename T, int TX, int R>
+inline cudaError_t launch_fused2_async_t(const Fused2Args<S, T> &a, cudaStream_t s)
+{
+    switch (kernel_flags(a)) {
+    case 0: return launch_fused2_async_f<S, T, TX, R, 0>(a, s);
+    case KF_FORCE: return launch_fused2_async_f<S, T, TX, R, KF_FORCE>(a, s);
+    case KF_SOLID: return launch_fused2_async_f<S, T, TX, R, KF_SOLID>(a, s);
+    default: return launch_fused2_async_f<S, T, TX, R, KF_FORCE | KF_SOLID>(a, s);
+    }
+}
+
+// the batched kernel always runs the general body (force and solids handled)
 template <typename S, typename T, int TX, int R> inline int async_resident_ctas()
 {
     using L = AsyncLayout<S, T, TX, R>;
-    static int per_sm = resident_ctas(k_batch2_async<S, T, TX, R>, TX, L::bytes);
+    static int per_sm =
+        resident_ctas(k_batch2_async<S, T, TX, R, KF_FORCE | KF_SOLID>, TX, L::bytes);
     return per_sm * sm_count();
 }
 
@@ -218,7 +228,8 @@ inline cudaError_t launch_batch2_async_t(const Fused2Args<S, T> *doms, const Ban
 {
     using L = AsyncLayout<S, T, TX, R>;
     if (async_resident_ctas<S, T, TX, R>() < 1) return cudaErrorInvalidConfiguration;
-    k_batch2_async<S, T, TX, R><<<grid, TX, L::bytes, s>>>(doms, tiles, ntiles, parity);
+    k_batch2_async<S, T, TX, R, KF_FORCE | KF_SOLID><<<grid, TX, L::bytes, s>>>(doms, tiles, ntiles,
+                                                                               parity);
     return cudaGetLastError();
 }
 

@@ -1,5 +1,6 @@
 // fused_step.cuh -- the fused Shan-Chen time step (kernel b) and the density
-// pass (kernel a), templated on storage type S and compute type T.
+// pass (kernel a), templated on storage type S, compute type T and the
+// specialisation flags (volume force present, solid nodes present).
 //
 // One launch performs one complete time step of the reference driver sequence
 //   compute_density x2            src/fluid.cpp:175-183
@@ -10,28 +11,38 @@
 //   stream(geom, f1, f2)          src/lbm.cpp:387-435
 // reading the populations once and writing them once.
 //
-// Tiling.  A CTA of TX threads owns W = TX-2 interior columns and tile_y rows.
-// Thread t handles column xb-1+t; threads 0 and TX-1 are halo columns that
-// only produce a density.  The CTA marches up its rows: in iteration r it loads
-// row r's populations (kept in registers), reduces them to the density, puts
-// density and mask into a 4-row shared-memory ring, synchronises once, then
-// collides row r-1 using the 3x3 density stencil from the ring and pushes the
-// post-collision populations to their destinations (half-way bounce-back at
-// solid neighbours).  Rows yb-1 and yb+tile_y are halo rows (density only).
-// Every destination slot has exactly one writer, so the kernel is race free
-// with separate input and output buffers.
+// Register-tile variant.  A CTA of TX threads owns W = TX-2 interior columns
+// and tile_y rows.  Thread t handles column xb-1+t; threads 0 and TX-1 are
+// halo columns that only produce a density.  The CTA marches up its rows: in
+// iteration r it loads row r's populations into registers, reduces them to the
+// density, puts density and mask into a 4-row shared-memory ring, synchronises
+// once, then collides row r-1 using the 3x3 density stencil from the ring and
+// pushes the post-collision populations to their destinations (half-way
+// bounce-back at solid neighbours).  Rows yb-1 and yb+tile_y are halo rows
+// (density only).  Every destination slot has exactly one writer, so the kernel
+// is race free with separate input and output buffers.
 //
 // FP64 (EXACT) follows the reference's operation order term by term and is
 // compiled with -fmad=false, so its populations are bit-identical to the
 // serial reference.  The shifted forms (T = float) store d_i = f_i - w_i*rho_ref
 // and evaluate the same physics in deviation form in FP32.
+//
+// Node indices are 32-bit (a lattice has fewer than 2^32 nodes); the per
+// population base pointers fout[k] + i*N depend only on kernel arguments, so
+// they are computed once per thread.
 #pragma once
 #include <cuda_fp16.h>
+
+#include <algorithm>
 
 #include "internal.h"
 #include "lattice.cuh"
 
 namespace sclbm {
+
+// specialisation flags of the fused kernels
+constexpr int KF_FORCE = 1; // a volume force is added to at least one component
+constexpr int KF_SOLID = 2; // the lattice has solid nodes
 
 template <typename S> struct Store;
 template <> struct Store<double> {
@@ -56,13 +67,7 @@ template <typename T> __device__ __forceinline__ bool rho_is_zero(T r)
     return a <= T(1e-16) * m;
 }
 
-// ---------------------------------------------------------------------------
-// exact FP64 node update (two components): reference operation order
-// ---------------------------------------------------------------------------
-struct NodeIn2 {
-    double f[2][9];
-};
-
+// exact FP64 equilibrium, src/fluid.cpp:254-276 (operation order kept)
 __device__ __forceinline__ void feq_exact(double r, double ux, double uy, double fe[9])
 {
     const double rt0 = w_eq(0) * r, rt1 = w_eq(1) * r, rt2 = w_eq(5) * r;
@@ -96,178 +101,205 @@ template <typename T> struct Stencil {
     int c;
 };
 
-// Collide node (x, yc) from its populations f and the density stencil, then
-// push the post-collision populations: the reference sequence of
-// src/lbm.cpp:177-204 (repulsive force), :250-269 (equilibrium velocity),
-// src/fluid.cpp:254-276 + src/lbm.cpp:305-311 (equilibrium, BGK),
-// :333-337 (volume force), :404-427 (stream with half-way bounce-back).
-// Push one post-collision population: to the neighbour along c_i when it is a
-// fluid node, else back into the opposite direction at the node itself.
-template <typename S, typename T>
-__device__ __forceinline__ void push_one(const Fused2Args<S, T> &a, const int k, const int i,
-                                         const T v, const bool nf, const size_t node, const int x,
-                                         const int xl, const int xr, const int yc, const int yd,
-                                         const int yu)
+// 32-bit indices of a node (nb[0]) and of its periodic neighbours along c_i
+struct Nbr {
+    uint32_t nb[9];
+};
+
+__device__ __forceinline__ Nbr make_nbr(const int nx, const int x, const int xl, const int xr,
+                                        const int yc, const int yd, const int yu)
 {
-    S *o = a.fout[k];
-    if (i == 0) {
-        Store<S>::st(o + node, v);
-    } else if (nf) {
-        const int xn = cx(i) == 0 ? x : (cx(i) > 0 ? xr : xl);
-        const int yn = cy(i) == 0 ? yc : (cy(i) > 0 ? yu : yd);
-        Store<S>::st(o + i * a.N + (size_t)yn * a.nx + xn, v);
-    } else {
-        Store<S>::st(o + opp(i) * a.N + node, v);
-    }
+    const uint32_t rc = (uint32_t)yc * (uint32_t)nx, rd = (uint32_t)yd * (uint32_t)nx,
+                   ru = (uint32_t)yu * (uint32_t)nx;
+    Nbr n;
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+        n.nb[i] = (cy(i) == 0 ? rc : (cy(i) > 0 ? ru : rd)) +
+                  (uint32_t)(cx(i) == 0 ? x : (cx(i) > 0 ? xr : xl));
+    return n;
 }
 
-// f[k][i] gives population i of component k (registers or shared memory).
-template <typename S, typename T, typename Pops>
+// Push one post-collision population: to the neighbour along c_i when it is a
+// fluid node, else back into the opposite direction at the node itself.
+template <typename S, typename T, bool SOLID>
+__device__ __forceinline__ void push_one(const Fused2Args<S, T> &a, const int k, const int i,
+                                         const T v, const bool nf, const Nbr &n)
+{
+    if (i == 0 || !SOLID || nf)
+        Store<S>::st(a.fout[k] + (size_t)i * a.N + n.nb[i], v);
+    else
+        Store<S>::st(a.fout[k] + (size_t)opp(i) * a.N + n.nb[0], v);
+}
+
+// Collide the node n.nb[0] from its populations f[k][i] (registers or shared
+// memory) and the density stencil, then push the results: the reference
+// sequence of src/lbm.cpp:177-204 (repulsive force), :250-269 (equilibrium
+// velocity), src/fluid.cpp:254-276 + src/lbm.cpp:305-311 (equilibrium, BGK),
+// :333-337 (volume force), :404-427 (stream with half-way bounce-back).
+template <typename S, typename T, int FLAGS, typename Pops>
 __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Pops &f,
-                                             const Stencil<T> &st, const int x, const int xl,
-                                             const int xr, const int yc, const int yd, const int yu)
+                                             const Stencil<T> &st, const Nbr &n)
 {
     constexpr bool EXACT = sizeof(T) == 8;
-    const size_t N = a.N;
-    const int nx = a.nx;
-    const size_t node = (size_t)yc * nx + x;
-    if (!st.m[1][st.c]) {
+    constexpr bool FORCE = (FLAGS & KF_FORCE) != 0, SOLID = (FLAGS & KF_SOLID) != 0;
+    const uint32_t node = n.nb[0];
+    if (SOLID && !st.m[1][st.c]) {
         // solid node: the reference's stream leaves zeros (src/lbm.cpp:431-434)
 #pragma unroll
         for (int k = 0; k < 2; ++k)
 #pragma unroll
-            for (int i = 0; i < 9; ++i) Store<S>::st(a.fout[k] + i * N + node, T(0));
-    } else {
-        bool nf[9];
-        T p0[9], p1[9];
+            for (int i = 0; i < 9; ++i) Store<S>::st(a.fout[k] + (size_t)i * a.N + node, T(0));
+        return;
+    }
+    bool nf[9];
+    T p0[9], p1[9];
+#pragma unroll
+    for (int i = 1; i < 9; ++i) {
+        const int sl = cy(i) + 1;
+        const int col = st.c + cx(i);
+        nf[i] = SOLID ? st.m[sl][col] != 0 : true;
+        p0[i] = st.r0[sl][col];
+        p1[i] = st.r1[sl][col];
+    }
+    nf[0] = true;
+    const T psi0 = st.r0[1][st.c], psi1 = st.r1[1][st.c];
+    if constexpr (EXACT) {
+        // repulsive force, src/lbm.cpp:177-204
+        double F0x = 0.0, F0y = 0.0, F1x = 0.0, F1y = 0.0, Sx = 0.0, Sy = 0.0;
 #pragma unroll
         for (int i = 1; i < 9; ++i) {
-            const int sl = cy(i) + 1;
-            const int col = st.c + cx(i);
-            nf[i] = st.m[sl][col] != 0;
-            p0[i] = st.r0[sl][col];
-            p1[i] = st.r1[sl][col];
-        }
-        const T psi0 = st.r0[1][st.c], psi1 = st.r1[1][st.c];
-        if constexpr (EXACT) {
-            // repulsive force, src/lbm.cpp:177-204
-            double F0x = 0.0, F0y = 0.0, F1x = 0.0, F1y = 0.0, Sx = 0.0, Sy = 0.0;
-#pragma unroll
-            for (int i = 1; i < 9; ++i) {
-                const double wcx = w_sc(i) * cx(i), wcy = w_sc(i) * cy(i);
-                if (nf[i]) {
-                    F0x += wcx * p1[i];
-                    F0y += wcy * p1[i];
-                    F1x += wcx * p0[i];
-                    F1y += wcy * p0[i];
-                } else {
-                    Sx += wcx; // solid sums, src/lbm.cpp:131-134
-                    Sy += wcy;
-                }
+            const double wcx = w_sc(i) * cx(i), wcy = w_sc(i) * cy(i);
+            if (nf[i]) {
+                F0x += wcx * p1[i];
+                F0y += wcy * p1[i];
+                F1x += wcx * p0[i];
+                F1y += wcy * p0[i];
+            } else {
+                Sx += wcx; // solid sums, src/lbm.cpp:131-134
+                Sy += wcy;
             }
-            F0x *= a.c[0].gf * psi0;
-            F0y *= a.c[0].gf * psi0;
-            F1x *= a.c[1].gf * psi1;
-            F1y *= a.c[1].gf * psi1;
-            // momentum, src/lbm.cpp:250-255
-            double j0x = 0.0, j0y = 0.0, j1x = 0.0, j1y = 0.0;
+        }
+        F0x *= a.c[0].gf * psi0;
+        F0y *= a.c[0].gf * psi0;
+        F1x *= a.c[1].gf * psi1;
+        F1y *= a.c[1].gf * psi1;
+        // momentum, src/lbm.cpp:250-255
+        double j0x = 0.0, j0y = 0.0, j1x = 0.0, j1y = 0.0;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            j0x += f[0][i] * double(cx(i));
+            j0y += f[0][i] * double(cy(i));
+            j1x += f[1][i] * double(cx(i));
+            j1y += f[1][i] * double(cy(i));
+        }
+        const double o0 = a.c[0].omega, o1 = a.c[1].omega;
+        const double ucx = (j0x * o0 + j1x * o1) / (psi0 * o0 + psi1 * o1);
+        const double ucy = (j0y * o0 + j1y * o1) / (psi0 * o0 + psi1 * o1);
+        const double psi[2] = {psi0, psi1};
+        const double Fx[2] = {F0x, F1x}, Fy[2] = {F0y, F1y};
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            double ux, uy;
+            if (!rho_is_zero(psi[k])) { // src/lbm.cpp:262-269
+                double fsx, fsy;
+                if (a.solid_from_mask) {
+                    fsx = a.c[k].gs_neg * Sx;
+                    fsy = a.c[k].gs_neg * Sy;
+                } else {
+                    fsx = a.fsx[k][node];
+                    fsy = a.fsy[k][node];
+                }
+                const double io = a.c[k].inv_omega;
+                ux = ucx + Fx[k] * io / psi[k] + fsx * io;
+                uy = ucy + Fy[k] * io / psi[k] + fsy * io;
+            } else {
+                ux = a.uex_old[k] ? a.uex_old[k][node] : 0.0;
+                uy = a.uey_old[k] ? a.uey_old[k][node] : 0.0;
+            }
+            double fe[9];
+            feq_exact(psi[k], ux, uy, fe);
+            const double om = a.c[k].omega, omm = a.c[k].one_m_omega;
 #pragma unroll
             for (int i = 0; i < 9; ++i) {
-                j0x += f[0][i] * double(cx(i));
-                j0y += f[0][i] * double(cy(i));
-                j1x += f[1][i] * double(cx(i));
-                j1y += f[1][i] * double(cy(i));
-            }
-            const double o0 = a.c[0].omega, o1 = a.c[1].omega;
-            const double ucx = (j0x * o0 + j1x * o1) / (psi0 * o0 + psi1 * o1);
-            const double ucy = (j0y * o0 + j1y * o1) / (psi0 * o0 + psi1 * o1);
-            const double psi[2] = {psi0, psi1};
-            const double Fx[2] = {F0x, F1x}, Fy[2] = {F0y, F1y};
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                double ux, uy;
-                if (!rho_is_zero(psi[k])) { // src/lbm.cpp:262-269
-                    double fsx, fsy;
-                    if (a.solid_from_mask) {
-                        fsx = a.c[k].gs_neg * Sx;
-                        fsy = a.c[k].gs_neg * Sy;
-                    } else {
-                        fsx = a.fsx[k][node];
-                        fsy = a.fsy[k][node];
-                    }
-                    const double io = a.c[k].inv_omega;
-                    ux = ucx + Fx[k] * io / psi[k] + fsx * io;
-                    uy = ucy + Fy[k] * io / psi[k] + fsy * io;
-                } else {
-                    ux = a.uex_old[k] ? a.uex_old[k][node] : 0.0;
-                    uy = a.uey_old[k] ? a.uey_old[k][node] : 0.0;
-                }
-                double fe[9];
-                feq_exact(psi[k], ux, uy, fe);
-                const double om = a.c[k].omega, omm = a.c[k].one_m_omega;
-#pragma unroll
-                for (int i = 0; i < 9; ++i) {
-                    double v = omm * f[k][i] + om * fe[i];
+                double v = omm * f[k][i] + om * fe[i];
+                if constexpr (FORCE) {
                     if (a.c[k].force_on) v += a.c[k].force[i];
-                    push_one<S, T>(a, k, i, v, nf[i], node, x, xl, xr, yc, yd, yu);
                 }
+                push_one<S, T, SOLID>(a, k, i, v, nf[i], n);
             }
+        }
+    } else {
+        // shifted form: the stencil holds rho - rho_ref
+        float A0x = 0.f, A0y = 0.f, A1x = 0.f, A1y = 0.f, Sx = 0.f, Sy = 0.f;
+#pragma unroll
+        for (int i = 1; i < 9; ++i) {
+            const float wcx = float(w_sc(i) * cx(i)), wcy = float(w_sc(i) * cy(i));
+            if (nf[i]) {
+                if (cx(i)) { A0x = fmaf(wcx, p1[i], A0x); A1x = fmaf(wcx, p0[i], A1x); }
+                if (cy(i)) { A0y = fmaf(wcy, p1[i], A0y); A1y = fmaf(wcy, p0[i], A1y); }
+            } else {
+                Sx += wcx;
+                Sy += wcy;
+            }
+        }
+        const float rr0 = a.c[0].rho_ref, rr1 = a.c[1].rho_ref;
+        const float r0 = rr0 + psi0, r1 = rr1 + psi1;
+        // sum over fluid neighbours of w c psi = A - rho_ref * S
+        float F0x, F0y, F1x, F1y;
+        if constexpr (SOLID) {
+            F0x = a.c[0].gf * r0 * fmaf(-rr1, Sx, A0x);
+            F0y = a.c[0].gf * r0 * fmaf(-rr1, Sy, A0y);
+            F1x = a.c[1].gf * r1 * fmaf(-rr0, Sx, A1x);
+            F1y = a.c[1].gf * r1 * fmaf(-rr0, Sy, A1y);
         } else {
-            // shifted form: the stencil holds rho - rho_ref
-            float A0x = 0.f, A0y = 0.f, A1x = 0.f, A1y = 0.f, Sx = 0.f, Sy = 0.f;
+            F0x = a.c[0].gf * r0 * A0x;
+            F0y = a.c[0].gf * r0 * A0y;
+            F1x = a.c[1].gf * r1 * A1x;
+            F1y = a.c[1].gf * r1 * A1y;
+        }
+        const T f01 = f[0][1], f03 = f[0][3], f05 = f[0][5], f06 = f[0][6], f07 = f[0][7], f08 = f[0][8];
+        const T f11 = f[1][1], f13 = f[1][3], f15 = f[1][5], f16 = f[1][6], f17 = f[1][7], f18 = f[1][8];
+        const float j0x = (f01 - f03) + (f05 - f06) + (f08 - f07);
+        const float j0y = (f[0][2] - f[0][4]) + (f05 + f06) - (f07 + f08);
+        const float j1x = (f11 - f13) + (f15 - f16) + (f18 - f17);
+        const float j1y = (f[1][2] - f[1][4]) + (f15 + f16) - (f17 + f18);
+        const float o0 = a.c[0].omega, o1 = a.c[1].omega;
+        const float inv_den = __fdividef(1.0f, fmaf(r0, o0, r1 * o1));
+        const float ucx = fmaf(j0x, o0, j1x * o1) * inv_den;
+        const float ucy = fmaf(j0y, o0, j1y * o1) * inv_den;
+        const float r[2] = {r0, r1}, dr[2] = {psi0, psi1};
+        const float Fx[2] = {F0x, F1x}, Fy[2] = {F0y, F1y};
 #pragma unroll
-            for (int i = 1; i < 9; ++i) {
-                const float wcx = float(w_sc(i) * cx(i)), wcy = float(w_sc(i) * cy(i));
-                if (nf[i]) {
-                    if (cx(i)) { A0x = fmaf(wcx, p1[i], A0x); A1x = fmaf(wcx, p0[i], A1x); }
-                    if (cy(i)) { A0y = fmaf(wcy, p1[i], A0y); A1y = fmaf(wcy, p0[i], A1y); }
-                } else {
-                    Sx += wcx;
-                    Sy += wcy;
-                }
-            }
-            const float rr0 = a.c[0].rho_ref, rr1 = a.c[1].rho_ref;
-            const float r0 = rr0 + psi0, r1 = rr1 + psi1;
-            // sum over fluid neighbours of w c psi = A - rho_ref * S
-            const float F0x = a.c[0].gf * r0 * fmaf(-rr1, Sx, A0x);
-            const float F0y = a.c[0].gf * r0 * fmaf(-rr1, Sy, A0y);
-            const float F1x = a.c[1].gf * r1 * fmaf(-rr0, Sx, A1x);
-            const float F1y = a.c[1].gf * r1 * fmaf(-rr0, Sy, A1y);
-            float j0x = (f[0][1] - f[0][3]) + (f[0][5] - f[0][6]) + (f[0][8] - f[0][7]);
-            float j0y = (f[0][2] - f[0][4]) + (f[0][5] + f[0][6]) - (f[0][7] + f[0][8]);
-            float j1x = (f[1][1] - f[1][3]) + (f[1][5] - f[1][6]) + (f[1][8] - f[1][7]);
-            float j1y = (f[1][2] - f[1][4]) + (f[1][5] + f[1][6]) - (f[1][7] + f[1][8]);
-            const float o0 = a.c[0].omega, o1 = a.c[1].omega;
-            const float inv_den = 1.0f / fmaf(r0, o0, r1 * o1);
-            const float ucx = fmaf(j0x, o0, j1x * o1) * inv_den;
-            const float ucy = fmaf(j0y, o0, j1y * o1) * inv_den;
-            const float r[2] = {r0, r1}, dr[2] = {psi0, psi1};
-            const float Fx[2] = {F0x, F1x}, Fy[2] = {F0y, F1y};
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                float ux = ucx, uy = ucy;
-                if (!rho_is_zero(r[k])) {
-                    const float io = a.c[k].inv_omega;
-                    const float ir = io / r[k];
+        for (int k = 0; k < 2; ++k) {
+            float ux = ucx, uy = ucy;
+            if (!rho_is_zero(r[k])) {
+                const float io = a.c[k].inv_omega;
+                const float ir = io * __fdividef(1.0f, r[k]);
+                if constexpr (SOLID) {
                     ux = fmaf(Fx[k], ir, fmaf(a.c[k].gs_neg * Sx, io, ucx));
                     uy = fmaf(Fy[k], ir, fmaf(a.c[k].gs_neg * Sy, io, ucy));
+                } else {
+                    ux = fmaf(Fx[k], ir, ucx);
+                    uy = fmaf(Fy[k], ir, ucy);
                 }
-                const float usq15 = 1.5f * fmaf(ux, ux, uy * uy);
-                const float om = a.c[k].omega;
+            }
+            const float usq15 = 1.5f * fmaf(ux, ux, uy * uy);
+            const float om = a.c[k].omega;
 #pragma unroll
-                for (int i = 0; i < 9; ++i) {
-                    const float fe = feq_dev(i, dr[k], r[k], ux, uy, usq15);
-                    const T fi = f[k][i];
-                    float v = fmaf(om, fe - fi, fi);
+            for (int i = 0; i < 9; ++i) {
+                const float fe = feq_dev(i, dr[k], r[k], ux, uy, usq15);
+                const T fi = f[k][i];
+                float v = fmaf(om, fe - fi, fi);
+                if constexpr (FORCE) {
                     if (a.c[k].force_on) v += a.c[k].force[i];
-                    push_one<S, T>(a, k, i, v, nf[i], node, x, xl, xr, yc, yd, yu);
                 }
+                push_one<S, T, SOLID>(a, k, i, v, nf[i], n);
             }
         }
     }
 }
 
-// shared-memory view of one node's populations in the ring: f[k][i]
+// shared-memory view of one node's populations in a ring: f[k][i]
 template <typename S, typename T, int P> struct RingPops {
     const S *base; // stage base + column
     struct Row {
@@ -278,17 +310,17 @@ template <typename S, typename T, int P> struct RingPops {
 };
 
 // ---------------------------------------------------------------------------
-// kernel b: fused two-component step
+// kernel b, register-tile variant
 // ---------------------------------------------------------------------------
 // One tile: interior columns [xb, xb+W) and rows [yb, yb+tile_y) of domain a.
-template <typename S, typename T, int TX, bool TWO_PASS>
+template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS>
 __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int xb, const int yb,
                                             T (&s_rho)[2][4][TX], uint8_t (&s_m)[4][TX])
 {
+    constexpr bool SOLID = (FLAGS & KF_SOLID) != 0;
     constexpr int W = TX - 2;
     const int t = threadIdx.x;
     const int nx = a.nx, ny = a.ny;
-    const size_t N = a.N;
     const int ncol = min(W, nx - xb);
     const int nrow = min(a.tile_y, ny - yb);
     const bool active = t <= ncol + 1;
@@ -296,26 +328,22 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
     const int x = wrap1(xb - 1 + t, nx);
     const int xl = wrap1(x - 1, nx), xr = wrap1(x + 1, nx);
 
-    T cur[2][9], prev[2][9];
-#pragma unroll
-    for (int k = 0; k < 2; ++k)
-#pragma unroll
-        for (int i = 0; i < 9; ++i) prev[k][i] = cur[k][i] = T(0);
-
-    for (int r = -1; r <= nrow; ++r) {
+    // one row: load row r into cur, publish its density, collide row r-1 (prev)
+    auto row = [&](const int r, T(&cur)[2][9], const T(&prev)[2][9]) {
         const int y = wrap1(yb + r, ny);
         const int slot = (r + 1) & 3;
         T rho[2] = {T(0), T(0)};
-        uint8_t m = 0;
+        uint8_t m = 1;
         if (active) {
-            const size_t node = (size_t)y * nx + x;
-            m = a.mask[node];
+            const uint32_t node = (uint32_t)y * (uint32_t)nx + (uint32_t)x;
+            if (SOLID) m = a.mask[node];
             const bool need_pops = !TWO_PASS || (interior && r >= 0 && r < nrow);
             if (need_pops) {
 #pragma unroll
                 for (int k = 0; k < 2; ++k)
 #pragma unroll
-                    for (int i = 0; i < 9; ++i) cur[k][i] = T(Store<S>::ld(a.fin[k] + i * N + node));
+                    for (int i = 0; i < 9; ++i)
+                        cur[k][i] = T(Store<S>::ld(a.fin[k] + (size_t)i * a.N + node));
             }
             if (TWO_PASS) {
                 rho[0] = a.rho_in[0][node];
@@ -329,7 +357,9 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
                     rho[k] = s;
                 }
             }
-            if (!m) rho[0] = rho[1] = T(0);
+            if (SOLID && !m) rho[0] = rho[1] = T(0);
+        } else {
+            m = 0;
         }
         s_rho[0][slot][t] = rho[0];
         s_rho[1][slot][t] = rho[1];
@@ -337,28 +367,35 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
         __syncthreads();
 
         if (r >= 1 && interior) {
-            // collide row r-1
             const int sc = r & 3, sm = (r - 1) & 3, sp = (r + 1) & 3;
             const int yc = wrap1(yb + r - 1, ny);
-            const int yd = wrap1(yc - 1, ny), yu = wrap1(yc + 1, ny);
             const Stencil<T> st{{s_rho[0][sm], s_rho[0][sc], s_rho[0][sp]},
                                 {s_rho[1][sm], s_rho[1][sc], s_rho[1][sp]},
                                 {s_m[sm], s_m[sc], s_m[sp]}, t};
-            collide_push<S, T>(a, prev, st, x, xl, xr, yc, yd, yu);
+            const Nbr n = make_nbr(nx, x, xl, xr, yc, wrap1(yc - 1, ny), wrap1(yc + 1, ny));
+            collide_push<S, T, FLAGS>(a, prev, st, n);
         }
+    };
+
+    T A[2][9], B[2][9];
 #pragma unroll
-        for (int k = 0; k < 2; ++k)
+    for (int k = 0; k < 2; ++k)
 #pragma unroll
-            for (int i = 0; i < 9; ++i) prev[k][i] = cur[k][i];
+        for (int i = 0; i < 9; ++i) A[k][i] = B[k][i] = T(0);
+    // two rows per trip so the buffers swap roles instead of being copied
+    for (int r = -1; r <= nrow; r += 2) {
+        row(r, A, B);
+        if (r + 1 <= nrow) row(r + 1, B, A);
     }
 }
 
-template <typename S, typename T, int TX, bool TWO_PASS>
+template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS>
 __global__ void __launch_bounds__(TX) k_fused2(const __grid_constant__ Fused2Args<S, T> a)
 {
     __shared__ T s_rho[2][4][TX];
     __shared__ uint8_t s_m[4][TX];
-    fused2_tile<S, T, TX, TWO_PASS>(a, blockIdx.x * (TX - 2), blockIdx.y * a.tile_y, s_rho, s_m);
+    fused2_tile<S, T, TX, TWO_PASS, FLAGS>(a, blockIdx.x * (TX - 2), blockIdx.y * a.tile_y, s_rho,
+                                           s_m);
 }
 
 // ---------------------------------------------------------------------------
@@ -460,16 +497,31 @@ __global__ void __launch_bounds__(256) k_density2(const uint8_t *__restrict__ ma
     }
 }
 
+// specialisation flags of an argument block
+template <typename S, typename T> inline int kernel_flags(const Fused2Args<S, T> &a)
+{
+    return (a.c[0].force_on || a.c[1].force_on ? KF_FORCE : 0) | (a.has_solid ? KF_SOLID : 0);
+}
+
+template <typename S, typename T, int TX, bool TWO, int FLAGS>
+inline cudaError_t launch_fused2_f(const Fused2Args<S, T> &a, cudaStream_t s)
+{
+    constexpr int W = TX - 2;
+    const dim3 grid((a.nx + W - 1) / W, (a.ny + a.tile_y - 1) / a.tile_y);
+    k_fused2<S, T, TX, TWO, FLAGS><<<grid, TX, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 template <typename S, typename T, int TX>
 inline cudaError_t launch_fused2_tx(const Fused2Args<S, T> &a, bool two_pass, cudaStream_t s)
 {
-    constexpr int W = TX - 2;
-    dim3 grid((a.nx + W - 1) / W, (a.ny + a.tile_y - 1) / a.tile_y);
-    if (two_pass)
-        k_fused2<S, T, TX, true><<<grid, TX, 0, s>>>(a);
-    else
-        k_fused2<S, T, TX, false><<<grid, TX, 0, s>>>(a);
-    return cudaGetLastError();
+    if (two_pass) return launch_fused2_f<S, T, TX, true, KF_FORCE | KF_SOLID>(a, s);
+    switch (kernel_flags(a)) {
+    case 0: return launch_fused2_f<S, T, TX, false, 0>(a, s);
+    case KF_FORCE: return launch_fused2_f<S, T, TX, false, KF_FORCE>(a, s);
+    case KF_SOLID: return launch_fused2_f<S, T, TX, false, KF_SOLID>(a, s);
+    default: return launch_fused2_f<S, T, TX, false, KF_FORCE | KF_SOLID>(a, s);
+    }
 }
 
 template <typename S, typename T>
@@ -478,11 +530,8 @@ inline cudaError_t launch_fused2_any(const Fused2Args<S, T> &a, int variant, int
 {
     if (a.tile_y < 1 || a.nx < 1 || a.ny < 1) return cudaErrorInvalidValue;
     const bool two = variant == 1;
-    switch (tx) {
-    case 64: return launch_fused2_tx<S, T, 64>(a, two, s);
-    case 256: return launch_fused2_tx<S, T, 256>(a, two, s);
-    default: return launch_fused2_tx<S, T, 128>(a, two, s);
-    }
+    if (tx == 64) return launch_fused2_tx<S, T, 64>(a, two, s);
+    return launch_fused2_tx<S, T, 128>(a, two, s);
 }
 
 } // namespace sclbm

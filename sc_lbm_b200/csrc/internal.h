@@ -52,6 +52,7 @@ struct sclbm_geometry {
     mutable uint8_t *d_mask = nullptr;
     mutable size_t d_count = 0;
     mutable bool dirty = true;
+    mutable bool has_solid = true; // refreshed with the device copy
 };
 
 struct sclbm_fluid {
@@ -90,6 +91,7 @@ template <typename S, typename T> struct Fused2Args {
     const T *rho_in[2];                  // two-pass variant: density per node
     CompParams<T> c[2];
     int solid_from_mask;                 // derive Fs from the mask (domain path)
+    int has_solid;                       // the mask has solid nodes (else all fluid)
 };
 
 // arguments of the single-component fused kernel

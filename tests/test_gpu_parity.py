@@ -68,7 +68,7 @@ def test_domain_fp64_bit_exact(sclbm, name):
     assert_golden(name, res, keys)
 
 
-@pytest.mark.parametrize("tx,tile_y,variant", [(64, 3, 2), (256, 8, 2), (128, 1, 2), (128, 5, 1),
+@pytest.mark.parametrize("tx,tile_y,variant", [(64, 3, 2), (128, 8, 2), (128, 1, 2), (128, 5, 1),
                                                (64, 64, 1), (128, 0, 0)])
 def test_domain_fp64_tiling_invariant(sclbm, tx, tile_y, variant):
     """Kernel variant (pipelined persistent, two pass, register tile) and tile

@@ -232,12 +232,14 @@ int sclbm_domain_step(sclbm_domain *d, int nsteps);
 /* Per component: total mass, x and y momentum over fluid nodes, reduced in
  * FP64 (out[3*comp + 0..2]); out[6] = number of non-finite populations. */
 int sclbm_domain_mass_momentum(sclbm_domain *d, double out[7]);
-/* Kernel selection (all variants give identical FP64 results):
- *   0 = single pass, persistent and load-balanced, population rows staged
- *       through a shared-memory ring by asynchronous copies (default; the
- *       FP16 form falls back to 2);
+/* Kernel selection (all variants give identical results):
+ *   0 = automatic (default): the fastest measured form for the storage
+ *       precision -- 3 for FP64, 2 for FP32 and FP16;
  *   1 = two pass (density kernel, then the fused kernel reading it);
- *   2 = single pass, one tile per CTA, rows held in registers.
+ *   2 = single pass, one tile per CTA, population rows held in registers;
+ *   3 = single pass, population rows staged through a shared-memory ring by
+ *       asynchronous copies, lattice cut into strips x row bands that are all
+ *       resident at once (FP64 and FP32 storage; FP16 uses 2).
  * tile_y = rows per tile of variants 1 and 2 (0 keeps the default). */
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y);
 /* Threads per tile of the register-tile kernel (variants 1, 2): 64 or 128. */
@@ -260,8 +262,10 @@ typedef struct sclbm_batch sclbm_batch;
 int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *tile_y_per_domain,
                        sclbm_batch **out);
 void sclbm_batch_destroy(sclbm_batch *b);
-/* Work decomposition: 0 = balanced row units over all domains (default for
- * FP64/FP32 storage), 2 = tile list with tile_y rows per tile (FP16). */
+/* Work decomposition (same results either way): 0 = automatic (3 for FP64
+ * storage, 2 otherwise); 2 = tile list, tile_y rows per tile, register-tile
+ * body; 3 = 128-column strips x row bands of one common height, pipelined
+ * body (FP64 and FP32 storage). */
 int sclbm_batch_set_kernel(sclbm_batch *b, int variant);
 /* advance every domain nsteps; use_graph = 1 replays a captured CUDA graph */
 int sclbm_batch_step(sclbm_batch *b, int nsteps, int use_graph);

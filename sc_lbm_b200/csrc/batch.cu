@@ -143,9 +143,11 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
     }
     // pipelined kernel: the smallest band height whose (domain, strip, band)
     // tiles all fit resident at once, bands of one domain split its rows evenly
-    b->use_units = b->prec != SCLBM_FP16_SHIFTED;
+    // default: bands for FP64 storage, tile list for FP32/FP16 (the faster form
+    // of each on B200); the FP16 form has no band kernel
+    b->use_units = b->prec == SCLBM_FP64;
     std::vector<BandTile> bands;
-    if (b->use_units) {
+    if (b->prec != SCLBM_FP16_SHIFTED) {
         const int res = std::max(1, b->prec == SCLBM_FP64 ? async_resident_fp64() : async_resident_f32());
         int H = 4;
         auto count = [&](int h) {
@@ -190,10 +192,11 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
 int sclbm_batch_set_kernel(sclbm_batch *b, int variant)
 {
     if (!b) return set_error(SCLBM_E_INVALID_ARGUMENT, "null batch");
-    if (variant != 0 && variant != 2) return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0 or 2");
-    if (variant == 0 && b->prec == SCLBM_FP16_SHIFTED)
+    if (variant != 0 && variant != 2 && variant != 3)
+        return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0, 2 or 3");
+    if (variant == 3 && b->prec == SCLBM_FP16_SHIFTED)
         return set_error(SCLBM_E_INVALID_ARGUMENT, "the FP16 form uses the tile list (variant 2)");
-    b->use_units = variant == 0;
+    b->use_units = variant == 3 || (variant == 0 && b->prec == SCLBM_FP64);
     for (auto &g : b->graph)
         if (g) {
             cudaGraphExecDestroy(g);

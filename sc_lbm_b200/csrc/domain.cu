@@ -173,11 +173,13 @@ __global__ void __launch_bounds__(256) k_monitor_final(int nblocks, const double
 int domain_default_tile_y(const sclbm_domain *d)
 {
     if (d->tile_y > 0) return d->tile_y;
+    // measured on B200 at 4096x4096 (register-tile kernel, 128 threads): 16 rows
+    // for FP32/FP64 storage, 32 for FP16; fewer rows when that leaves too few
+    // tiles to occupy every SM at least twice
     const int W = d->tx - 2;
     const long tiles_x = (long)((d->nx + W - 1) / W);
-    // aim for several waves of CTAs over the SMs, with 8..64 rows per tile
-    long ty = (long)d->ny * tiles_x / ((long)sm_count() * 8);
-    ty = std::max(8L, std::min(64L, ty));
+    long ty = d->prec == SCLBM_FP16_SHIFTED ? 32 : 16;
+    while (ty > 4 && tiles_x * (((long)d->ny + ty - 1) / ty) < 2L * sm_count()) ty /= 2;
     return (int)ty;
 }
 
@@ -252,11 +254,14 @@ static cudaError_t step_one(const sclbm_domain *d, cudaStream_t s)
                                    (float *)d->rho_tmp[1], d->N, s);
         if (e != cudaSuccess) return e;
     }
-    if (d->variant == 0) { // pipelined persistent single pass (FP64 / FP32 storage)
+    // variant 0 picks the fastest measured form: pipelined for FP64 storage,
+    // register tile for FP32/FP16; 3 forces the pipelined kernel
+    const bool pipelined = d->variant == 3 || (d->variant == 0 && sizeof(S) == 8);
+    if (pipelined) {
         if constexpr (sizeof(S) == 8) return launch_fused2_async_fp64(a, s);
         else if constexpr (sizeof(S) == 4) return launch_fused2_async_f32(a, s);
     }
-    // variant 1: two pass; variant 2 (and FP16): register-tile single pass
+    // variant 1: two pass; variant 2 (and the FP16 form): register-tile single pass
     const int v = d->variant == 1 ? 1 : 0;
     if constexpr (sizeof(S) == 8) return launch_fused2_fp64(a, v, d->tx, s);
     else if constexpr (sizeof(S) == 4) return launch_fused2_f32(a, v, d->tx, s);
@@ -367,7 +372,7 @@ fail:
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y)
 {
     if (!d) return set_error(SCLBM_E_INVALID_ARGUMENT, "null domain");
-    if (variant < 0 || variant > 2) return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0, 1 or 2");
+    if (variant < 0 || variant > 3) return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0..3");
     if (tile_y < 0 || tile_y > 4096) return set_error(SCLBM_E_INVALID_ARGUMENT, "bad tile_y");
     if (variant == 1 && !d->rho_tmp[0] && d->ncomp == 2) {
         const size_t es = d->prec == SCLBM_FP64 ? 8 : 4;

@@ -246,6 +246,25 @@ int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y);
 int sclbm_domain_set_threads(sclbm_domain *d, int tx);
 /* Device bytes held by the domain. */
 size_t sclbm_domain_device_bytes(const sclbm_domain *d);
+/* Allocation-free form of sclbm_domain_mass_momentum.  No counterpart in the
+ * reference.  For callers that may not allocate device memory -- a host
+ * program that gives the library a fixed arena and forbids further
+ * cudaMalloc, or code running where allocation is not permitted -- it works
+ * on buffers the caller already owns: f0/f1 are device pointers to the
+ * populations in the domain layout (9N values of the storage type of
+ * `precision`, deviations from w_i*rho_ref[k] for the shifted forms), mask a
+ * device pointer to N bytes (1 fluid, 0 solid).  Its scratch is a fixed
+ * file-scope device array (about 128 KB, held on every GPU that loads the
+ * library until exit), which limits the lattice to 2^27 nodes (e.g.
+ * 16384 x 8192); larger lattices return SCLBM_E_INVALID_ARGUMENT.  The first
+ * call on a device looks up the array's device address, so make that first
+ * call before any stream capture.  All calls share the array and it keeps
+ * the last call's partial sums; calls that overlap on the GPU race.  Work
+ * runs on `cuda_stream` (NULL = the default stream), which is synchronised
+ * before out[7] (as sclbm_domain_mass_momentum) is returned. */
+int sclbm_mass_momentum_noalloc(const void *f0, const void *f1, const uint8_t *mask, size_t nx,
+                                size_t ny, int ncomp, int precision, const double *rho_ref,
+                                void *cuda_stream, double out[7]);
 /* One end-to-end call: upload both components' populations from host memory,
  * advance nsteps, return the densities to host memory. f2/rho2 are ignored
  * for one component. */

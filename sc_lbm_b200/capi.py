@@ -116,6 +116,8 @@ SIGNATURES = {
     "sclbm_domain_set_threads": (C.c_int, [_VP, C.c_int]),
     "sclbm_domain_device_bytes": (_SZ, [_VP]),
     "sclbm_domain_run": (C.c_int, [_VP, _D, _D, C.c_int, _D, _D]),
+    "sclbm_mass_momentum_noalloc": (C.c_int, [_VP, _VP, _VP, _SZ, _SZ, C.c_int, C.c_int, _D, _VP,
+                                              _D]),
     "sclbm_batch_create": (C.c_int, [C.POINTER(_VP), C.c_int, C.POINTER(C.c_int), C.POINTER(_VP)]),
     "sclbm_batch_destroy": (None, [_VP]),
     "sclbm_batch_step": (C.c_int, [_VP, C.c_int, C.c_int]),

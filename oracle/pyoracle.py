@@ -315,10 +315,14 @@ def read_ref_output(path: str) -> dict:
     return out
 
 
-def run_ref(case) -> dict:
-    """Run a case through the compiled reference (oracle/_ref)."""
-    if not have_ref():
-        raise FileNotFoundError("oracle/_ref/sclbm_ref_runner was not built")
+def run_ref(case, runner: str | None = None) -> dict:
+    """Run a case through the compiled reference (oracle/_ref), or through
+    ``runner``: the same driver source (ref_runner.cpp) built against another
+    implementation of the reference's Geometry / Fluid / LBM classes."""
+    if runner is None:
+        if not have_ref():
+            raise FileNotFoundError("oracle/_ref/sclbm_ref_runner was not built")
+        runner = REF_RUNNER
     with tempfile.TemporaryDirectory() as td:
         init_path = os.path.join(td, "init.bin")
         out_path = os.path.join(td, "out.bin")
@@ -327,7 +331,7 @@ def run_ref(case) -> dict:
             np.asarray(case["init"][1], dtype="<f8").tofile(init_path)
         with open(spec, "w") as fh:
             fh.write(_spec_text(case, init_path, out_path))
-        subprocess.run([REF_RUNNER, "case", spec], check=True, stdout=subprocess.DEVNULL)
+        subprocess.run([runner, "case", spec], check=True, stdout=subprocess.DEVNULL)
         return read_ref_output(out_path)
 
 

@@ -61,13 +61,17 @@ def measured_peak_hbm():
 
 
 def ncu_traffic(kernel_key):
-    """DRAM bytes per launch from the committed ncu summary, if one exists."""
-    p = os.path.join(ROOT, "profiles", "traffic.json")
-    if not os.path.exists(p):
-        return None
-    with open(p) as fh:
-        d = json.load(fh)
-    return d.get(kernel_key)
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
+    the committed ncu summaries: a line `traffic_per_launch[<key>] = <bytes>`."""
+    import glob
+    import re
+    pat = re.compile(r"^traffic_per_launch\[(\w+)\]\s*=\s*(\d+)\s*$", re.M)
+    for p in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        with open(p) as fh:
+            for key, val in pat.findall(fh.read()):
+                if key == kernel_key:
+                    return int(val)
+    return None
 
 
 class ClockSampler:
@@ -369,10 +373,12 @@ def run_ours(args):
                      "bytes_per_update": B_LU["fp32s"], "peak_source": peak_kind},
         "fp64": {"value": round(mlups64, 2), "unit": "MLUPS", "ms_per_step": round(ms64, 5),
                  "frac": round(B_LU["fp64"] * N / (ms64 * 1e-3) / 1e9 / peak, 4),
+                 "traffic": ncu_traffic("fused_fp64_4096"),
                  "speedup_fp32s_over_fp64": round(mlups32 / mlups64, 3)},
         "fp16": {"value": round(world * N / (ms16 * 1e-3) / 1e6, 2), "unit": "MLUPS",
                  "ms_per_step": round(ms16, 5),
-                 "frac": round(B_LU["fp16s"] * N / (ms16 * 1e-3) / 1e9 / peak, 4)},
+                 "frac": round(B_LU["fp16s"] * N / (ms16 * 1e-3) / 1e9 / peak, 4),
+                 "traffic": ncu_traffic("fused_fp16s_4096")},
         "accuracy": accuracy,
         "e2e": {"value": round(e2e_mlups, 2), "unit": "MLUPS",
                 "h2d_bytes_per_step": 2 * 9 * N * 8, "d2h_bytes_per_step": 2 * N * 8,

@@ -277,18 +277,30 @@ int sclbm_domain_run(sclbm_domain *d, const double *f1, const double *f2, int ns
  * sequence of a run is captured in a CUDA graph. */
 typedef struct sclbm_batch sclbm_batch;
 
-/* tile_y_per_domain may be NULL (rows per tile chosen by size class) */
+/* tile_y_per_domain may be NULL: rows per tile then come from the tuned table
+ * (sclbm_tuned_config) for each domain's size class */
 int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *tile_y_per_domain,
                        sclbm_batch **out);
 void sclbm_batch_destroy(sclbm_batch *b);
-/* Work decomposition (same results either way): 0 = automatic (3 for FP64
- * storage, 2 otherwise); 2 = tile list, tile_y rows per tile, register-tile
- * body; 3 = 128-column strips x row bands of one common height, pipelined
- * body (FP64 and FP32 storage). */
+/* Work decomposition (same results either way): 0 = automatic (the tuned
+ * variant of the size class holding most of the batch's nodes); 2 = tile
+ * list, tile_y rows per tile, register-tile body; 3 = 128-column strips x
+ * row bands of one common height, pipelined body (FP64 and FP32 storage). */
 int sclbm_batch_set_kernel(sclbm_batch *b, int variant);
 /* advance every domain nsteps; use_graph = 1 replays a captured CUDA graph */
 int sclbm_batch_step(sclbm_batch *b, int nsteps, int use_graph);
 int sclbm_batch_info(const sclbm_batch *b, int *ntiles, int *grid_ctas);
+
+/* Tuned launch shape for an nx x ny two-component domain stored at
+ * `precision` (sclbm_precision; -1 = the recommended one), from the table
+ * that sc_lbm_b200/autotune.py measured on B200 and the build compiled in.
+ * Sizes outside the table take the nearest size class.  *recommended is the
+ * fastest storage whose density error against FP64 stayed within 1e-5 for
+ * that class.  Host-only lookup (no device needed).  No reference
+ * counterpart: the reference has no batched or tuned path.  Any output
+ * pointer may be NULL. */
+int sclbm_tuned_config(size_t nx, size_t ny, int precision, int *tile_y, int *variant,
+                       int *recommended);
 
 #ifdef __cplusplus
 }

@@ -313,6 +313,15 @@ class Batch(_Handle):
         return a.value, b.value
 
 
+def tuned_config(nx: int, ny: int, precision: int | None = None) -> dict:
+    """Tuned batch launch shape for an nx x ny domain (host lookup in the
+    autotuned table): {"tile_y", "variant", "recommended_precision"}."""
+    t, v, r = C.c_int(), C.c_int(), C.c_int()
+    call("sclbm_tuned_config", int(nx), int(ny), -1 if precision is None else int(precision),
+         C.byref(t), C.byref(v), C.byref(r))
+    return {"tile_y": t.value, "variant": v.value, "recommended_precision": r.value}
+
+
 def synchronize():
     call("sclbm_synchronize")
 

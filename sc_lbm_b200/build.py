@@ -17,11 +17,47 @@ HOST = os.path.join(HERE, "host")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libsclbm_b200.so")
 
+GEN = os.path.join(BUILD, "gen")
+TUNING_JSON = os.path.join(HERE, "tuning", "b200.json")
+TUNED_HEADER = os.path.join(GEN, "sclbm_tuned_table.h")
+
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
-          f"-I{os.path.join(ROOT, 'include')}", f"-I{os.path.join(HOST, 'include')}"]
+          f"-I{os.path.join(ROOT, 'include')}", f"-I{os.path.join(HOST, 'include')}", f"-I{GEN}"]
 EXACT = {"ops_fp64.cu"}
+PRECISIONS = ("fp64", "fp32s", "fp16s")  # sclbm_precision order
+
+
+def tuned_table_source(path: str = TUNING_JSON) -> str:
+    """C table of the autotuner's size classes (empty when no results exist)."""
+    import json
+    lines = [f"// generated by sc_lbm_b200/build.py from {os.path.relpath(path, ROOT)}",
+             "#pragma once", "// included after tuning.h (SclbmTunedClass)"]
+    classes = []
+    if os.path.exists(path):
+        with open(path) as fh:
+            classes = json.load(fh).get("classes", [])
+    rows = []
+    for c in classes:
+        shapes = ", ".join("{%d, %d}" % (int(c["shapes"][p]["variant"]), int(c["shapes"][p]["tile_y"]))
+                           for p in PRECISIONS)
+        rows.append("    {%d, %d, %d, %d, %d, {%s}}," % (c["nx"][0], c["nx"][1], c["ny"][0], c["ny"][1],
+                                                      PRECISIONS.index(c["precision"]), shapes))
+    lines.append(f"#define SCLBM_TUNED_COUNT {len(rows)}")
+    lines.append("static const SclbmTunedClass kSclbmTuned[%d] = {" % max(1, len(rows)))
+    lines += rows or ["    {0, 0, 0, 0, 0, {{0, 0}, {0, 0}, {0, 0}}},"]
+    lines.append("};")
+    return "\n".join(lines) + "\n"
+
+
+def _gen_tuning_header():
+    os.makedirs(GEN, exist_ok=True)
+    src = tuned_table_source()
+    old = open(TUNED_HEADER).read() if os.path.exists(TUNED_HEADER) else None
+    if src != old:
+        with open(TUNED_HEADER, "w") as fh:
+            fh.write(src)
 
 
 def _sources():
@@ -35,7 +71,7 @@ def _sources():
 
 
 def _headers():
-    hs = [os.path.join(ROOT, "include", "sclbm.h")]
+    hs = [os.path.join(ROOT, "include", "sclbm.h"), TUNED_HEADER]
     for d in (CSRC, os.path.join(HOST, "include")):
         for r, _, fs in os.walk(d):
             hs += [os.path.join(r, f) for f in fs if f.endswith((".h", ".cuh"))]
@@ -51,6 +87,7 @@ def _stale(out, deps):
 
 def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
+    _gen_tuning_header()
     headers = _headers()
     objs = []
     for src in _sources():

@@ -123,6 +123,8 @@ SIGNATURES = {
     "sclbm_batch_step": (C.c_int, [_VP, C.c_int, C.c_int]),
     "sclbm_batch_set_kernel": (C.c_int, [_VP, C.c_int]),
     "sclbm_batch_info": (C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "sclbm_tuned_config": (C.c_int, [_SZ, _SZ, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int)]),
 }
 
 _lib = None

@@ -3,20 +3,23 @@
 // CUDA graph and replayed.  All domains of a batch share the storage precision
 // and the buffer parity.  Two work decompositions:
 //
-//  * bands (default for FP64/FP32): every domain is cut into 128-column strips
-//    and row bands of one common height, chosen as the smallest for which all
+//  * bands (FP64/FP32): every domain is cut into 128-column strips and row
+//    bands of one common height, chosen as the smallest for which all
 //    (domain, strip, band) tiles are resident at once; neighbouring strips of
 //    a band are adjacent in the list so they walk the same rows together; the
 //    pipelined single-pass body (fused_async.cuh) runs each tile;
-//  * tile list (FP16, or on request): every tile (126 columns x tile_y rows)
-//    of every domain, largest first; CTA b takes tiles b, b+grid, ... and runs
-//    the register-tile body (batch_kernel.cuh).
+//  * tile list: every tile (126 columns x tile_y rows) of every domain,
+//    largest first; CTA b takes tiles b, b+grid, ... and runs the
+//    register-tile body (batch_kernel.cuh).
+// The automatic choice and the rows per tile come from the autotuned size-class
+// table (tuning.h), weighted by the nodes of each class in the batch.
 #include <algorithm>
 #include <numeric>
 
 #include "domain.h"
 #include "batch_kernel.cuh"
 #include "fused_async.cuh"
+#include "tuning.h"
 
 
 using namespace sclbm;
@@ -32,6 +35,7 @@ struct sclbm_batch {
     int nbands = 0, band_grid = 0, band_rows = 0;
     int ntiles = 0, grid = 0, parity = 0;
     int use_units = 1;
+    int auto_units = 1; // tuned choice for variant 0
     cudaGraphExec_t graph[2] = {nullptr, nullptr}; // by starting parity
     cudaStream_t graph_stream = nullptr;
 };
@@ -106,11 +110,16 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
     auto *b = new (std::nothrow) sclbm_batch();
     if (!b) return set_error(SCLBM_E_ALLOC, "host allocation failed");
     b->doms.assign(domains, domains + ndomains);
+    if (!b->doms[0]) {
+        delete b;
+        return set_error(SCLBM_E_INVALID_ARGUMENT, "null domain in batch");
+    }
     b->prec = b->doms[0]->prec;
     b->parity = b->doms[0]->parity;
     std::vector<int> ty(ndomains);
     std::vector<TileRef> tiles;
     std::vector<long> cost;
+    double nodes_units = 0.0, nodes_tiles = 0.0;
     const int W = BATCH_TX - 2;
     for (int k = 0; k < ndomains; ++k) {
         sclbm_domain *d = b->doms[k];
@@ -119,7 +128,9 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
             return set_error(SCLBM_E_INVALID_ARGUMENT,
                              "batch domains must be two-component, of one precision and in step");
         }
-        ty[k] = tile_y_per_domain && tile_y_per_domain[k] > 0 ? tile_y_per_domain[k] : 16;
+        const SclbmTunedShape ts = tuned_shape(d->nx, d->ny, b->prec);
+        ty[k] = tile_y_per_domain && tile_y_per_domain[k] > 0 ? tile_y_per_domain[k] : ts.tile_y;
+        (ts.variant == 3 ? nodes_units : nodes_tiles) += (double)d->nx * (double)d->ny;
         for (int yb = 0; yb < (int)d->ny; yb += ty[k])
             for (int xb = 0; xb < (int)d->nx; xb += W) {
                 tiles.push_back(TileRef{k, xb, yb, 0});
@@ -142,10 +153,11 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
     default: rc = upload_args<__half, float>(b, ty); break;
     }
     // pipelined kernel: the smallest band height whose (domain, strip, band)
-    // tiles all fit resident at once, bands of one domain split its rows evenly
-    // default: bands for FP64 storage, tile list for FP32/FP16 (the faster form
-    // of each on B200); the FP16 form has no band kernel
-    b->use_units = b->prec == SCLBM_FP64;
+    // tiles all fit resident at once, bands of one domain split its rows evenly.
+    // Default: the tuned variant of the size classes holding most nodes (the
+    // FP16 form has no band kernel)
+    b->auto_units = b->prec != SCLBM_FP16_SHIFTED && nodes_units > nodes_tiles;
+    b->use_units = b->auto_units;
     std::vector<BandTile> bands;
     if (b->prec != SCLBM_FP16_SHIFTED) {
         const int res = std::max(1, b->prec == SCLBM_FP64 ? async_resident_fp64() : async_resident_f32());
@@ -196,7 +208,7 @@ int sclbm_batch_set_kernel(sclbm_batch *b, int variant)
         return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0, 2 or 3");
     if (variant == 3 && b->prec == SCLBM_FP16_SHIFTED)
         return set_error(SCLBM_E_INVALID_ARGUMENT, "the FP16 form uses the tile list (variant 2)");
-    b->use_units = variant == 3 || (variant == 0 && b->prec == SCLBM_FP64);
+    b->use_units = variant == 3 || (variant == 0 && b->auto_units);
     for (auto &g : b->graph)
         if (g) {
             cudaGraphExecDestroy(g);

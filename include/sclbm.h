@@ -223,6 +223,16 @@ void sclbm_domain_destroy(sclbm_domain *d);
 /* populations of component comp in reference layout (FP64, 9N values) */
 int sclbm_domain_upload_f(sclbm_domain *d, int comp, const double *f, size_t count);
 int sclbm_domain_download_f(sclbm_domain *d, int comp, double *f, size_t count);
+/* Seeded initial state written on the device, for lattices whose FP64
+ * populations are too large to build on the host: f_i = rho/9 on fluid nodes
+ * and 0 on solids (the shape of LBM::initialize_droplet, src/lbm.cpp:11-48,
+ * and Fluid::simple_ini, src/fluid.cpp:64-104), rho = rho0*(1 + amp*(2u-1)),
+ * u in [0,1) the splitmix64 uniform of (seed, node index).  Equal bit for bit
+ * to uploading the same state built on the host (sc_lbm_b200/workloads.py
+ * draws the same stream).  Replaces building the state through get_f_dist();
+ * no reference counterpart (the reference's perturbed init,
+ * src/fluid.cpp:107-151, is unseeded). */
+int sclbm_domain_init_noise(sclbm_domain *d, int comp, double rho0, double amp, uint64_t seed);
 /* density (Fluid::compute_density) and velocity (Fluid::compute_velocities) */
 int sclbm_domain_download_rho(sclbm_domain *d, int comp, double *rho, size_t count);
 int sclbm_domain_download_velocity(sclbm_domain *d, int comp, double *ux, double *uy,

@@ -253,6 +253,11 @@ class Domain(_Handle):
         v = np.ascontiguousarray(f, dtype=np.float64).ravel()
         call("sclbm_domain_upload_f", self._h, comp, _dp(v), v.size)
 
+    def init_noise(self, comp, rho0, amp, seed):
+        """f_i = rho/9, rho = rho0*(1 + amp*(2u-1)), u = splitmix64(seed, node),
+        written on the device (equal to uploading workloads.populations)."""
+        call("sclbm_domain_init_noise", self._h, int(comp), float(rho0), float(amp), int(seed))
+
     def download_f(self, comp) -> np.ndarray:
         out = np.empty(9 * self.N)
         call("sclbm_domain_download_f", self._h, comp, _dp(out), out.size)

@@ -108,6 +108,7 @@ SIGNATURES = {
     "sclbm_domain_destroy": (None, [_VP]),
     "sclbm_domain_upload_f": (C.c_int, [_VP, C.c_int, _D, _SZ]),
     "sclbm_domain_download_f": (C.c_int, [_VP, C.c_int, _D, _SZ]),
+    "sclbm_domain_init_noise": (C.c_int, [_VP, C.c_int, C.c_double, C.c_double, C.c_uint64]),
     "sclbm_domain_download_rho": (C.c_int, [_VP, C.c_int, _D, _SZ]),
     "sclbm_domain_download_velocity": (C.c_int, [_VP, C.c_int, _D, _D, _SZ]),
     "sclbm_domain_step": (C.c_int, [_VP, C.c_int]),

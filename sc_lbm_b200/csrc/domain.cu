@@ -46,6 +46,41 @@ __global__ void k_upload_dir(size_t N, const uint8_t *__restrict__ mask,
     GRID_STRIDE(n, N) { dst[n] = Conv<S>::from_f64(mask[n] ? src[n] - shift : 0.0); }
 }
 
+// Seeded initial state written on the device: f_i = rho/9 on fluid nodes (the
+// reference initialisers' shape, src/lbm.cpp:11-48, src/fluid.cpp:64-104),
+// rho = rho0 * (1 + amp * (2u - 1)) with u the splitmix64 uniform of
+// (seed, node) -- the stream of the host generator sc_lbm_b200/workloads.py,
+// operation for operation in round-to-nearest (no contraction), so the state
+// equals the host-built one bit for bit; storage conversion as in
+// k_upload_dir (shift[i] = w_i * rho_ref, 0 for the FP64 form).
+struct InitShift {
+    double s[9];
+};
+
+__device__ inline double splitmix_u01(unsigned long long seed, unsigned long long n)
+{
+    unsigned long long z = n + seed * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z = z ^ (z >> 31);
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+template <typename S>
+__global__ void k_init_noise(size_t N, const uint8_t *__restrict__ mask, S *__restrict__ f,
+                             double rho0, double amp, unsigned long long seed, InitShift sh)
+{
+    GRID_STRIDE(n, N)
+    {
+        const double u = splitmix_u01(seed, n);
+        const double r = __dmul_rn(rho0, __dadd_rn(1.0, __dmul_rn(amp, __dsub_rn(__dmul_rn(2.0, u), 1.0))));
+        const double fi = __ddiv_rn(r, 9.0);
+        const bool fluid = mask[n] != 0;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) f[i * N + n] = Conv<S>::from_f64(fluid ? __dsub_rn(fi, sh.s[i]) : 0.0);
+    }
+}
+
 // storage -> staging (FP64 f_i); solid nodes read 0 in the shifted forms
 template <typename S>
 __global__ void k_download_dir(size_t N, const uint8_t *__restrict__ mask, const S *__restrict__ src,
@@ -427,6 +462,32 @@ int sclbm_domain_upload_f(sclbm_domain *d, int comp, const double *f, size_t cou
             SCLBM_LAUNCHED("upload conversion");
         }
     }
+    SCLBM_CUDA(cudaStreamSynchronize(s));
+    return SCLBM_OK;
+}
+
+int sclbm_domain_init_noise(sclbm_domain *d, int comp, double rho0, double amp, uint64_t seed)
+{
+    int rc = check_comp(d, comp, 0, 0);
+    if (rc) return rc;
+    if (!std::isfinite(rho0) || !std::isfinite(amp))
+        return set_error(SCLBM_E_INVALID_ARGUMENT, "non-finite density or amplitude");
+    cudaStream_t s = stream();
+    InitShift sh;
+    for (int i = 0; i < 9; ++i) sh.s[i] = d->prec == SCLBM_FP64 ? 0.0 : w_eq(i) * d->p.rho_ref[comp];
+    void *dst = d->buf[d->parity][comp];
+    const int grid = grid_for(d->N, 256);
+    switch (d->prec) {
+    case SCLBM_FP64:
+        k_init_noise<double><<<grid, 256, 0, s>>>(d->N, d->d_mask, (double *)dst, rho0, amp, seed, sh);
+        break;
+    case SCLBM_FP32_SHIFTED:
+        k_init_noise<float><<<grid, 256, 0, s>>>(d->N, d->d_mask, (float *)dst, rho0, amp, seed, sh);
+        break;
+    default:
+        k_init_noise<__half><<<grid, 256, 0, s>>>(d->N, d->d_mask, (__half *)dst, rho0, amp, seed, sh);
+    }
+    SCLBM_LAUNCHED("seeded initial state");
     SCLBM_CUDA(cudaStreamSynchronize(s));
     return SCLBM_OK;
 }

@@ -128,6 +128,10 @@ def single_cases() -> dict:
     c["poiseuille_200x50"] = dict(nx=200, ny=50, geom=[("walls", 1, "x")], mode="single",
                                   fluid1=(1.0, 0, 0), init=("simple", 1.0),
                                   force=(1, force_vec(1e-6, "x")), steps=100)
+    # Poiseuille channel at the full length of the measurement plan (10,000 steps)
+    c["poiseuille_200x50_10k"] = dict(nx=200, ny=50, geom=[("walls", 1, "x")], mode="single",
+                                      fluid1=(1.0, 0, 0), init=("simple", 1.0),
+                                      force=(1, force_vec(1e-6, "x")), steps=10000)
     c["ops1_y_walls_20x10"] = dict(nx=20, ny=10, geom=[("walls", 3, "y")], mode="ops1",
                                    fluid1=(1.0, 0, 0),
                                    init=("file", noisy_f(3, 20, 10, 1.0, 0.05)),

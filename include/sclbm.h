@@ -249,8 +249,10 @@ int sclbm_domain_mass_momentum(sclbm_domain *d, double out[7]);
  *   2 = single pass, one tile per CTA, population rows held in registers;
  *   3 = single pass, population rows staged through a shared-memory ring by
  *       asynchronous copies, lattice cut into strips x row bands that are all
- *       resident at once (FP64 and FP32 storage; FP16 uses 2).
- * tile_y = rows per tile of variants 1 and 2 (0 keeps the default). */
+ *       resident at once (FP64 and FP32 storage; FP16 uses 2);
+ *   4 = variant 2 with the row segments of each tile prefetched into L2 two
+ *       rows ahead (cp.async.bulk.prefetch), 128 threads per tile.
+ * tile_y = rows per tile of variants 1, 2 and 4 (0 keeps the default). */
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y);
 /* Threads per tile of the register-tile kernel (variants 1, 2): 64 or 128. */
 int sclbm_domain_set_threads(sclbm_domain *d, int tx);

@@ -14,19 +14,32 @@ struct TileRef {
     int dom, xb, yb, pad;
 };
 
-// doms holds two argument blocks per domain (buffer parity 0 and 1)
+// doms holds two argument blocks per domain (buffer parity 0 and 1).  The
+// block of the current tile's domain is copied into shared memory, so the tile
+// body reads its fields from there instead of holding the whole block in
+// registers.
 template <typename S, typename T>
-__global__ void __launch_bounds__(BATCH_TX)
+__global__ void __launch_bounds__(BATCH_TX, sizeof(T) == 8 ? 1 : 6)
     k_batch2(const Fused2Args<S, T> *__restrict__ doms, const TileRef *__restrict__ tiles,
              int ntiles, int parity)
 {
     __shared__ T s_rho[2][4][BATCH_TX];
     __shared__ uint8_t s_m[4][BATCH_TX];
+    __shared__ __align__(16) Fused2Args<S, T> sa;
+    static_assert(sizeof(Fused2Args<S, T>) % 4 == 0, "argument block copied as words");
+    int loaded = -1;
     for (int i = blockIdx.x; i < ntiles; i += gridDim.x) {
         const TileRef tr = tiles[i];
-        const Fused2Args<S, T> a = doms[2 * tr.dom + parity];
-        fused2_tile<S, T, BATCH_TX, false, KF_FORCE | KF_SOLID>(a, tr.xb, tr.yb, s_rho, s_m);
-        __syncthreads(); // the shared ring is reused by the next tile
+        const int key = 2 * tr.dom + parity;
+        if (key != loaded) { // uniform over the CTA
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(doms + key);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(&sa);
+            for (int w = threadIdx.x; w < (int)(sizeof(sa) / 4); w += BATCH_TX) dst[w] = src[w];
+            __syncthreads();
+            loaded = key;
+        }
+        fused2_tile<S, T, BATCH_TX, false, KF_FORCE | KF_SOLID>(sa, tr.xb, tr.yb, s_rho, s_m);
+        __syncthreads(); // the shared ring and block are reused by the next tile
     }
 }
 

@@ -695,6 +695,7 @@ int sclbm_lbm_step(sclbm_lbm *l, const sclbm_geometry *g, sclbm_fluid *f1, sclbm
     }
     a.solid_from_mask = 0;
     a.has_solid = g->has_solid ? 1 : 0;
+    a.solids_zero = 0; // caller-owned arrays: solid nodes are rewritten with zeros
     for (int s = 0; s < nsteps; ++s) {
         a.fin[0] = f1->d[SCLBM_FIELD_F];
         a.fin[1] = f2->d[SCLBM_FIELD_F];

@@ -81,6 +81,18 @@ __global__ void k_init_noise(size_t N, const uint8_t *__restrict__ mask, S *__re
     }
 }
 
+// all nine populations of the solid nodes set to 0 (FP64 uploads)
+__global__ void k_zero_solids(size_t N, const uint8_t *__restrict__ mask, double *__restrict__ f)
+{
+    GRID_STRIDE(n, N)
+    {
+        if (!mask[n]) {
+#pragma unroll
+            for (int i = 0; i < 9; ++i) f[i * N + n] = 0.0;
+        }
+    }
+}
+
 // storage -> staging (FP64 f_i); solid nodes read 0 in the shifted forms
 template <typename S>
 __global__ void k_download_dir(size_t N, const uint8_t *__restrict__ mask, const S *__restrict__ src,
@@ -248,6 +260,7 @@ static void fill2(const sclbm_domain *d, Fused2Args<S, T> &a)
     }
     a.solid_from_mask = 1;
     a.has_solid = d->has_solid ? 1 : 0;
+    a.solids_zero = 1; // creation, uploads and initialisers write 0 at solid nodes
 }
 
 void domain_fused2_args(const sclbm_domain *d, Fused2Args<double, double> *a64,
@@ -296,8 +309,9 @@ static cudaError_t step_one(const sclbm_domain *d, cudaStream_t s)
         if constexpr (sizeof(S) == 8) return launch_fused2_async_fp64(a, s);
         else if constexpr (sizeof(S) == 4) return launch_fused2_async_f32(a, s);
     }
-    // variant 1: two pass; variant 2 (and the FP16 form): register-tile single pass
-    const int v = d->variant == 1 ? 1 : 0;
+    // variant 1: two pass; 4: register tile with L2 row prefetch; variant 2
+    // (and the FP16 form): register-tile single pass
+    const int v = d->variant == 1 ? 1 : (d->variant == 4 ? 4 : 0);
     if constexpr (sizeof(S) == 8) return launch_fused2_fp64(a, v, d->tx, s);
     else if constexpr (sizeof(S) == 4) return launch_fused2_f32(a, v, d->tx, s);
     else return launch_fused2_f16(a, v, d->tx, s);
@@ -407,7 +421,7 @@ fail:
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y)
 {
     if (!d) return set_error(SCLBM_E_INVALID_ARGUMENT, "null domain");
-    if (variant < 0 || variant > 3) return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0..3");
+    if (variant < 0 || variant > 4) return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0..4");
     if (tile_y < 0 || tile_y > 4096) return set_error(SCLBM_E_INVALID_ARGUMENT, "bad tile_y");
     if (variant == 1 && !d->rho_tmp[0] && d->ncomp == 2) {
         const size_t es = d->prec == SCLBM_FP64 ? 8 : 4;
@@ -449,6 +463,12 @@ int sclbm_domain_upload_f(sclbm_domain *d, int comp, const double *f, size_t cou
     void *dst = d->buf[d->parity][comp];
     if (d->prec == SCLBM_FP64) {
         SCLBM_CUDA(cudaMemcpyAsync(dst, f, 9 * d->N * 8, cudaMemcpyHostToDevice, s));
+        if (d->has_solid) {
+            // solid nodes hold 0 in both buffers (what the reference's stream leaves
+            // there after every step); the fused kernels rely on it
+            k_zero_solids<<<grid_for(d->N, 256), 256, 0, s>>>(d->N, d->d_mask, (double *)dst);
+            SCLBM_LAUNCHED("solid zeroing");
+        }
     } else {
         const double rr = d->p.rho_ref[comp];
         for (int i = 0; i < 9; ++i) {

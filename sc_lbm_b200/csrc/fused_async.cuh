@@ -168,10 +168,21 @@ __global__ void __launch_bounds__(TX)
                    int ntiles, int parity)
 {
     extern __shared__ __align__(16) unsigned char smem[];
+    // argument block of the current tile's domain, read from shared memory
+    __shared__ __align__(16) Fused2Args<S, T> sa;
+    static_assert(sizeof(Fused2Args<S, T>) % 4 == 0, "argument block copied as words");
+    int loaded = -1;
     for (int i = blockIdx.x; i < ntiles; i += gridDim.x) {
         const BandTile tl = tiles[i];
-        const Fused2Args<S, T> a = doms[2 * tl.dom + parity];
-        async_segment<S, T, TX, R, FLAGS>(a, tl.xb, tl.y0, tl.y1, smem);
+        const int key = 2 * tl.dom + parity;
+        if (key != loaded) { // uniform over the CTA; the previous segment ended in a barrier
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(doms + key);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(&sa);
+            for (int w = threadIdx.x; w < (int)(sizeof(sa) / 4); w += TX) dst[w] = src[w];
+            __syncthreads();
+            loaded = key;
+        }
+        async_segment<S, T, TX, R, FLAGS>(sa, tl.xb, tl.y0, tl.y1, smem);
     }
 }
 

@@ -58,6 +58,14 @@ template <> struct Store<__half> {
     static __device__ __forceinline__ void st(__half *p, float v) { *p = __float2half_rn(v); }
 };
 
+// Bulk prefetch of [p, p + bytes) into L2 (p and bytes multiples of 16): one
+// instruction brings a whole row segment of a population array closer before
+// the per-thread loads of a later row iteration ask for it.
+__device__ __forceinline__ void prefetch_l2_bulk(const void *p, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // equal_floats(r, 0.0, 1e-16) of include/utils.h:145-150
 template <typename T> __device__ __forceinline__ bool rho_is_zero(T r)
 {
@@ -144,11 +152,14 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
     constexpr bool FORCE = (FLAGS & KF_FORCE) != 0, SOLID = (FLAGS & KF_SOLID) != 0;
     const uint32_t node = n.nb[0];
     if (SOLID && !st.m[1][st.c]) {
-        // solid node: the reference's stream leaves zeros (src/lbm.cpp:431-434)
+        // solid node: the reference's stream leaves zeros (src/lbm.cpp:431-434);
+        // on the domain path both buffers already hold them
+        if (!a.solids_zero) {
 #pragma unroll
-        for (int k = 0; k < 2; ++k)
+            for (int k = 0; k < 2; ++k)
 #pragma unroll
-            for (int i = 0; i < 9; ++i) Store<S>::st(a.fout[k] + (size_t)i * a.N + node, T(0));
+                for (int i = 0; i < 9; ++i) Store<S>::st(a.fout[k] + (size_t)i * a.N + node, T(0));
+        }
         return;
     }
     bool nf[9];
@@ -313,7 +324,12 @@ template <typename S, typename T, int P> struct RingPops {
 // kernel b, register-tile variant
 // ---------------------------------------------------------------------------
 // One tile: interior columns [xb, xb+W) and rows [yb, yb+tile_y) of domain a.
-template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS>
+// PF: threads 0..17 prefetch, PF_DIST rows ahead, the row segments of the 18
+// population arrays into L2 (cp.async.bulk.prefetch), so the row loads of the
+// later iteration find them there.
+constexpr int PF_DIST = 2;
+
+template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS, bool PF = false>
 __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int xb, const int yb,
                                             T (&s_rho)[2][4][TX], uint8_t (&s_m)[4][TX])
 {
@@ -332,12 +348,26 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
     auto row = [&](const int r, T(&cur)[2][9], const T(&prev)[2][9]) {
         const int y = wrap1(yb + r, ny);
         const int slot = (r + 1) & 3;
+        if constexpr (PF) {
+            const int rp = r + PF_DIST;
+            if (t < 18 && rp <= nrow) {
+                const int k = t >= 9 ? 1 : 0, i = t - 9 * k;
+                const S *arr = a.fin[k] + (size_t)i * a.N + (size_t)wrap1(yb + rp, ny) * (size_t)nx;
+                const uintptr_t lo = (uintptr_t)(arr + max(xb - 1, 0)) & ~uintptr_t(15);
+                const uintptr_t end = (uintptr_t)(a.fin[k] + 9 * a.N) & ~uintptr_t(15);
+                const uintptr_t up = ((uintptr_t)(arr + min(xb + ncol + 1, nx)) + 15) & ~uintptr_t(15);
+                const uintptr_t hi = up < end ? up : end;
+                if (hi > lo) prefetch_l2_bulk((const void *)lo, (uint32_t)(hi - lo));
+            }
+        }
         T rho[2] = {T(0), T(0)};
         uint8_t m = 1;
         if (active) {
             const uint32_t node = (uint32_t)y * (uint32_t)nx + (uint32_t)x;
             if (SOLID) m = a.mask[node];
-            const bool need_pops = !TWO_PASS || (interior && r >= 0 && r < nrow);
+            // solid nodes hold zeros on the domain path: nothing to read there
+            const bool need_pops = (!TWO_PASS || (interior && r >= 0 && r < nrow)) &&
+                                   (!SOLID || m || !a.solids_zero);
             if (need_pops) {
 #pragma unroll
                 for (int k = 0; k < 2; ++k)
@@ -389,13 +419,15 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
     }
 }
 
-template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS>
-__global__ void __launch_bounds__(TX) k_fused2(const __grid_constant__ Fused2Args<S, T> a)
+// FP32 arithmetic: capped at 80 registers so six 128-thread CTAs are resident
+// per SM (the solid and force paths fit without spilling)
+template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS, bool PF = false>
+__global__ void __launch_bounds__(TX, sizeof(T) == 8 ? 1 : 6) k_fused2(const __grid_constant__ Fused2Args<S, T> a)
 {
     __shared__ T s_rho[2][4][TX];
     __shared__ uint8_t s_m[4][TX];
-    fused2_tile<S, T, TX, TWO_PASS, FLAGS>(a, blockIdx.x * (TX - 2), blockIdx.y * a.tile_y, s_rho,
-                                           s_m);
+    fused2_tile<S, T, TX, TWO_PASS, FLAGS, PF>(a, blockIdx.x * (TX - 2), blockIdx.y * a.tile_y,
+                                               s_rho, s_m);
 }
 
 // ---------------------------------------------------------------------------
@@ -503,27 +535,29 @@ template <typename S, typename T> inline int kernel_flags(const Fused2Args<S, T>
     return (a.c[0].force_on || a.c[1].force_on ? KF_FORCE : 0) | (a.has_solid ? KF_SOLID : 0);
 }
 
-template <typename S, typename T, int TX, bool TWO, int FLAGS>
+template <typename S, typename T, int TX, bool TWO, int FLAGS, bool PF = false>
 inline cudaError_t launch_fused2_f(const Fused2Args<S, T> &a, cudaStream_t s)
 {
     constexpr int W = TX - 2;
     const dim3 grid((a.nx + W - 1) / W, (a.ny + a.tile_y - 1) / a.tile_y);
-    k_fused2<S, T, TX, TWO, FLAGS><<<grid, TX, 0, s>>>(a);
+    k_fused2<S, T, TX, TWO, FLAGS, PF><<<grid, TX, 0, s>>>(a);
     return cudaGetLastError();
 }
 
-template <typename S, typename T, int TX>
+template <typename S, typename T, int TX, bool PF = false>
 inline cudaError_t launch_fused2_tx(const Fused2Args<S, T> &a, bool two_pass, cudaStream_t s)
 {
     if (two_pass) return launch_fused2_f<S, T, TX, true, KF_FORCE | KF_SOLID>(a, s);
     switch (kernel_flags(a)) {
-    case 0: return launch_fused2_f<S, T, TX, false, 0>(a, s);
-    case KF_FORCE: return launch_fused2_f<S, T, TX, false, KF_FORCE>(a, s);
-    case KF_SOLID: return launch_fused2_f<S, T, TX, false, KF_SOLID>(a, s);
-    default: return launch_fused2_f<S, T, TX, false, KF_FORCE | KF_SOLID>(a, s);
+    case 0: return launch_fused2_f<S, T, TX, false, 0, PF>(a, s);
+    case KF_FORCE: return launch_fused2_f<S, T, TX, false, KF_FORCE, PF>(a, s);
+    case KF_SOLID: return launch_fused2_f<S, T, TX, false, KF_SOLID, PF>(a, s);
+    default: return launch_fused2_f<S, T, TX, false, KF_FORCE | KF_SOLID, PF>(a, s);
     }
 }
 
+// variant 1: two pass; 4: single pass with L2 row prefetch (128 threads);
+// otherwise the single-pass register tile
 template <typename S, typename T>
 inline cudaError_t launch_fused2_any(const Fused2Args<S, T> &a, int variant, int tx,
                                      cudaStream_t s)
@@ -531,6 +565,7 @@ inline cudaError_t launch_fused2_any(const Fused2Args<S, T> &a, int variant, int
     if (a.tile_y < 1 || a.nx < 1 || a.ny < 1) return cudaErrorInvalidValue;
     const bool two = variant == 1;
     if (tx == 64) return launch_fused2_tx<S, T, 64>(a, two, s);
+    if (variant == 4) return launch_fused2_tx<S, T, 128, true>(a, false, s);
     return launch_fused2_tx<S, T, 128>(a, two, s);
 }
 

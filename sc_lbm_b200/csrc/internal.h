@@ -92,6 +92,8 @@ template <typename S, typename T> struct Fused2Args {
     CompParams<T> c[2];
     int solid_from_mask;                 // derive Fs from the mask (domain path)
     int has_solid;                       // the mask has solid nodes (else all fluid)
+    int solids_zero;                     // both buffers hold 0 at solid nodes: the kernels
+                                         // neither read nor write them (domain path)
 };
 
 // arguments of the single-component fused kernel

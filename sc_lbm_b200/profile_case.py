@@ -30,23 +30,49 @@ def main():
     ap.add_argument("--variant", type=int, default=0)
     ap.add_argument("--tile-y", type=int, default=0)
     ap.add_argument("--threads", type=int, default=128)
+    ap.add_argument("--porosity", type=float, default=1.0,
+                    help="< 1: seeded disks of radius 8-20 and walls top and bottom")
+    ap.add_argument("--force", action="store_true", help="body force 1e-5 along x on component 1")
+    ap.add_argument("--ensemble", type=int, default=0,
+                    help="> 0: time a batch of that many seeded ensemble domains instead")
     args = ap.parse_args()
 
     import torch
     import sc_lbm_b200 as sc
+    from sc_lbm_b200 import workloads as W
 
     prec = {"fp64": sc.FP64, "fp32": sc.FP32_SHIFTED, "fp16": sc.FP16_SHIFTED}[args.precision]
-    N = args.nx * args.ny
-    rng = np.random.default_rng(1)
-    f = [np.tile((1.0 + 0.02 * (rng.random(N) - 0.5)) / 9.0, 9) for _ in range(2)]
     stream = torch.cuda.Stream()
     sc.set_stream(stream.cuda_stream)
-    d = sc.Domain(args.nx, args.ny, np.ones(N, np.int32),
-                  sc.make_params(ncomp=2, g_fluid=(1.2, 1.2), rho_ref=(1.0, 1.0)), prec)
-    d.set_kernel(args.variant, args.tile_y)
-    d.set_threads(args.threads)
-    d.upload_f(0, f[0])
-    d.upload_f(1, f[1])
+    if args.ensemble > 0:
+        members = W.ensemble(args.ensemble)
+        doms = []
+        for m in members:
+            dm = sc.Domain(m["nx"], m["ny"], m["mask"], W.params_of(m, sc), prec)
+            dm.upload_f(0, m["f1"])
+            dm.upload_f(1, m["f2"])
+            doms.append(dm)
+        N = sum(dm.N for dm in doms)
+        d = sc.Batch(doms)
+        if args.variant:
+            d.set_kernel(args.variant)
+    else:
+        N = args.nx * args.ny
+        if args.porosity < 1.0:
+            mask, _, _ = W.disk_mask(args.nx, args.ny, args.porosity, 8, 20, 11, walls="x")
+        else:
+            mask = np.ones(N, np.int32)
+        rng = np.random.default_rng(1)
+        f = [W.populations(1.0 + 0.02 * (rng.random(N) - 0.5), mask) for _ in range(2)]
+        d = sc.Domain(args.nx, args.ny, mask,
+                      sc.make_params(ncomp=2, g_fluid=(1.2, 1.2), g_solid=(-0.2, 0.2),
+                                     rho_ref=(1.0, 1.0),
+                                     force=(W.force_vec(1e-5) if args.force else None, None)),
+                      prec)
+        d.set_kernel(args.variant, args.tile_y)
+        d.set_threads(args.threads)
+        d.upload_f(0, f[0])
+        d.upload_f(1, f[1])
     d.step(args.warmup)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -56,7 +82,8 @@ def main():
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / max(args.steps, 1)
     print(json.dumps({"nx": args.nx, "ny": args.ny, "precision": args.precision,
-                      "variant": args.variant, "ms_per_step": ms,
+                      "variant": args.variant, "porosity": args.porosity, "force": args.force,
+                      "ensemble": args.ensemble, "nodes": N, "ms_per_step": ms,
                       "mlups": N / (ms * 1e-3) / 1e6}))
 
 

@@ -69,10 +69,11 @@ def test_domain_fp64_bit_exact(sclbm, name):
 
 
 @pytest.mark.parametrize("tx,tile_y,variant", [(64, 3, 2), (128, 8, 2), (128, 1, 2), (128, 5, 1),
-                                               (64, 64, 1), (128, 0, 0), (128, 0, 3)])
+                                               (64, 64, 1), (128, 0, 0), (128, 0, 3), (128, 0, 4),
+                                               (128, 3, 4)])
 def test_domain_fp64_tiling_invariant(sclbm, tx, tile_y, variant):
-    """Kernel variant (pipelined persistent, two pass, register tile) and tile
-    shape do not change a single bit."""
+    """Kernel variant (pipelined persistent, two pass, register tile, register
+    tile with L2 prefetch) and tile shape do not change a single bit."""
     for name in ("porous_96x48", "spinodal_48x40", "channel_80x32", "droplet_solid_flow"):
         res = gpu_runner.run_domain(sclbm, RUNS[name], sclbm.FP64, variant=variant,
                                     tile_y=tile_y, tx=tx)
@@ -143,11 +144,15 @@ def test_shifted_forms_density_error(sclbm, oracle, name, steps, prec, tol_max, 
         assert e_max <= tol_max and e_l2 <= tol_l2, (name, prec, c, e_max, e_l2)
 
 
-def test_shifted_two_pass_matches_single_pass(sclbm):
+@pytest.mark.parametrize("variant,tile_y", [(1, 4), (4, 0), (4, 7), (3, 0)])
+def test_shifted_variants_match_register_tile(sclbm, variant, tile_y):
+    """The shifted forms give the same bytes with every kernel variant."""
     for prec in (sclbm.FP32_SHIFTED, sclbm.FP16_SHIFTED):
+        if variant == 3 and prec == sclbm.FP16_SHIFTED:
+            continue
         a = gpu_runner.run_domain(sclbm, RUNS["porous_96x48"], prec, rho_ref=(0.5, 1.5))
         b = gpu_runner.run_domain(sclbm, RUNS["porous_96x48"], prec, rho_ref=(0.5, 1.5),
-                                  variant=1, tile_y=4)
+                                  variant=variant, tile_y=tile_y)
         assert a["c1_f"].tobytes() == b["c1_f"].tobytes()
         assert a["c2_f"].tobytes() == b["c2_f"].tobytes()
 

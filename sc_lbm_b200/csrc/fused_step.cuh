@@ -344,6 +344,11 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
     const int x = wrap1(xb - 1 + t, nx);
     const int xl = wrap1(x - 1, nx), xr = wrap1(x + 1, nx);
 
+    // the mask of the next row is loaded one iteration ahead, so the population
+    // loads of a row never wait on its mask load
+    uint8_t m_ahead = 1;
+    if (SOLID && active) m_ahead = a.mask[(uint32_t)wrap1(yb - 1, ny) * (uint32_t)nx + (uint32_t)x];
+
     // one row: load row r into cur, publish its density, collide row r-1 (prev)
     auto row = [&](const int r, T(&cur)[2][9], const T(&prev)[2][9]) {
         const int y = wrap1(yb + r, ny);
@@ -364,7 +369,11 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
         uint8_t m = 1;
         if (active) {
             const uint32_t node = (uint32_t)y * (uint32_t)nx + (uint32_t)x;
-            if (SOLID) m = a.mask[node];
+            if (SOLID) {
+                m = m_ahead;
+                if (r < nrow)
+                    m_ahead = a.mask[(uint32_t)wrap1(yb + r + 1, ny) * (uint32_t)nx + (uint32_t)x];
+            }
             // solid nodes hold zeros on the domain path: nothing to read there
             const bool need_pops = (!TWO_PASS || (interior && r >= 0 && r < nrow)) &&
                                    (!SOLID || m || !a.solids_zero);

@@ -220,14 +220,30 @@ __global__ void __launch_bounds__(256) k_monitor_final(int nblocks, const double
 int domain_default_tile_y(const sclbm_domain *d)
 {
     if (d->tile_y > 0) return d->tile_y;
-    // measured on B200 at 4096x4096 (register-tile kernel, 128 threads): 16 rows
-    // for FP32/FP64 storage, 32 for FP16; fewer rows when that leaves too few
-    // tiles to occupy every SM at least twice
+    // Measured on B200 at 4096x4096 (register-tile kernel, 128 threads): 16 rows
+    // for FP32/FP64 storage, 32 for FP16.  With fewer than ~8 waves of tiles the
+    // last partial wave costs a visible share, so the rows per tile are chosen
+    // to minimise waves x (rows + 2 halo rows), the time model of one launch.
     const int W = d->tx - 2;
     const long tiles_x = (long)((d->nx + W - 1) / W);
-    long ty = d->prec == SCLBM_FP16_SHIFTED ? 32 : 16;
-    while (ty > 4 && tiles_x * (((long)d->ny + ty - 1) / ty) < 2L * sm_count()) ty /= 2;
-    return (int)ty;
+    const long base = d->prec == SCLBM_FP16_SHIFTED ? 32 : 16;
+    // resident 128-thread CTAs per SM: 6 for the FP32-arithmetic kernels (80
+    // registers), 3 for FP64 (168 registers)
+    const long per_sm = d->tx == 64 ? (d->prec == SCLBM_FP64 ? 6 : 10) : (d->prec == SCLBM_FP64 ? 3 : 6);
+    const long R = per_sm * sm_count();
+    auto tiles = [&](long ty) { return tiles_x * (((long)d->ny + ty - 1) / ty); };
+    if (tiles(base) >= 8 * R) return (int)base;
+    static const long cand[] = {4, 6, 8, 10, 12, 16, 20, 24, 32};
+    long best = base, best_cost = -1;
+    for (long ty : cand) {
+        if (ty > std::max<long>(base, 4) && ty > (long)d->ny) continue;
+        const long cost = ((tiles(ty) + R - 1) / R) * (ty + 2);
+        if (best_cost < 0 || cost < best_cost || (cost == best_cost && ty > best)) {
+            best = ty;
+            best_cost = cost;
+        }
+    }
+    return (int)best;
 }
 
 template <typename T> static void fill_comp(CompParams<T> &c, const sclbm_params &p, int k)

@@ -128,15 +128,19 @@ __device__ __forceinline__ Nbr make_nbr(const int nx, const int x, const int xl,
 }
 
 // Push one post-collision population: to the neighbour along c_i when it is a
-// fluid node, else back into the opposite direction at the node itself.
+// fluid node, else back into the opposite direction at the node itself.  The
+// destination is selected, not branched on, so warps with both kinds of
+// nodes issue one store per population.
 template <typename S, typename T, bool SOLID>
 __device__ __forceinline__ void push_one(const Fused2Args<S, T> &a, const int k, const int i,
                                          const T v, const bool nf, const Nbr &n)
 {
-    if (i == 0 || !SOLID || nf)
+    if (i == 0 || !SOLID) {
         Store<S>::st(a.fout[k] + (size_t)i * a.N + n.nb[i], v);
-    else
-        Store<S>::st(a.fout[k] + (size_t)opp(i) * a.N + n.nb[0], v);
+    } else {
+        const size_t off = nf ? (size_t)i * a.N + n.nb[i] : (size_t)opp(i) * a.N + n.nb[0];
+        Store<S>::st(a.fout[k] + off, v);
+    }
 }
 
 // Collide the node n.nb[0] from its populations f[k][i] (registers or shared
@@ -176,19 +180,18 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
     const T psi0 = st.r0[1][st.c], psi1 = st.r1[1][st.c];
     if constexpr (EXACT) {
         // repulsive force, src/lbm.cpp:177-204
+        // (selects, not branches: the sums take exactly the reference's terms)
         double F0x = 0.0, F0y = 0.0, F1x = 0.0, F1y = 0.0, Sx = 0.0, Sy = 0.0;
 #pragma unroll
         for (int i = 1; i < 9; ++i) {
             const double wcx = w_sc(i) * cx(i), wcy = w_sc(i) * cy(i);
-            if (nf[i]) {
-                F0x += wcx * p1[i];
-                F0y += wcy * p1[i];
-                F1x += wcx * p0[i];
-                F1y += wcy * p0[i];
-            } else {
-                Sx += wcx; // solid sums, src/lbm.cpp:131-134
-                Sy += wcy;
-            }
+            const bool f = nf[i];
+            F0x = f ? F0x + wcx * p1[i] : F0x;
+            F0y = f ? F0y + wcy * p1[i] : F0y;
+            F1x = f ? F1x + wcx * p0[i] : F1x;
+            F1y = f ? F1y + wcy * p0[i] : F1y;
+            Sx = f ? Sx : Sx + wcx; // solid sums, src/lbm.cpp:131-134
+            Sy = f ? Sy : Sy + wcy;
         }
         F0x *= a.c[0].gf * psi0;
         F0y *= a.c[0].gf * psi0;
@@ -240,17 +243,17 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
             }
         }
     } else {
-        // shifted form: the stencil holds rho - rho_ref
+        // shifted form: the stencil holds rho - rho_ref, and 0 at solid nodes, so
+        // the sums over fluid neighbours run over all neighbours without tests
         float A0x = 0.f, A0y = 0.f, A1x = 0.f, A1y = 0.f, Sx = 0.f, Sy = 0.f;
 #pragma unroll
         for (int i = 1; i < 9; ++i) {
             const float wcx = float(w_sc(i) * cx(i)), wcy = float(w_sc(i) * cy(i));
-            if (nf[i]) {
-                if (cx(i)) { A0x = fmaf(wcx, p1[i], A0x); A1x = fmaf(wcx, p0[i], A1x); }
-                if (cy(i)) { A0y = fmaf(wcy, p1[i], A0y); A1y = fmaf(wcy, p0[i], A1y); }
-            } else {
-                Sx += wcx;
-                Sy += wcy;
+            if (cx(i)) { A0x = fmaf(wcx, p1[i], A0x); A1x = fmaf(wcx, p0[i], A1x); }
+            if (cy(i)) { A0y = fmaf(wcy, p1[i], A0y); A1y = fmaf(wcy, p0[i], A1y); }
+            if constexpr (SOLID) {
+                if (cx(i)) Sx += nf[i] ? 0.f : wcx;
+                if (cy(i)) Sy += nf[i] ? 0.f : wcy;
             }
         }
         const float rr0 = a.c[0].rho_ref, rr1 = a.c[1].rho_ref;

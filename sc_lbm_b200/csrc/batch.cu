@@ -36,6 +36,7 @@ struct sclbm_batch {
     int ntiles = 0, grid = 0, parity = 0;
     int use_units = 1;
     int auto_units = 1; // tuned choice for variant 0
+    int ahead = 0, grid_ahead = 0; // tile list with the load-ahead body (variant 5)
     cudaGraphExec_t graph[2] = {nullptr, nullptr}; // by starting parity
     cudaStream_t graph_stream = nullptr;
 };
@@ -54,10 +55,10 @@ static cudaError_t batch_launch_any(sclbm_batch *b, int parity, cudaStream_t s)
                                  b->ntiles, parity, b->grid, s);
     case SCLBM_FP32_SHIFTED:
         return launch_batch_f32((const Fused2Args<float, float> *)b->d_args, b->d_tiles,
-                                b->ntiles, parity, b->grid, s);
+                                b->ntiles, parity, b->ahead ? b->grid_ahead : b->grid, b->ahead, s);
     default:
         return launch_batch_f16((const Fused2Args<__half, float> *)b->d_args, b->d_tiles,
-                                b->ntiles, parity, b->grid, s);
+                                b->ntiles, parity, b->ahead ? b->grid_ahead : b->grid, b->ahead, s);
     }
 }
 
@@ -147,6 +148,10 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
     int per_sm = batch_blocks_per_sm(b->prec);
     if (per_sm < 1) per_sm = 1;
     b->grid = std::max(1, std::min(b->ntiles, per_sm * sm_count()));
+    if (b->prec != SCLBM_FP64) {
+        const int pa = std::max(1, batch_blocks_per_sm(b->prec, true));
+        b->grid_ahead = std::max(1, std::min(b->ntiles, pa * sm_count()));
+    }
     switch (b->prec) {
     case SCLBM_FP64: rc = upload_args<double, double>(b, ty); break;
     case SCLBM_FP32_SHIFTED: rc = upload_args<float, float>(b, ty); break;
@@ -204,11 +209,14 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
 int sclbm_batch_set_kernel(sclbm_batch *b, int variant)
 {
     if (!b) return set_error(SCLBM_E_INVALID_ARGUMENT, "null batch");
-    if (variant != 0 && variant != 2 && variant != 3)
-        return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0, 2 or 3");
+    if (variant != 0 && variant != 2 && variant != 3 && variant != 5)
+        return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0, 2, 3 or 5");
     if (variant == 3 && b->prec == SCLBM_FP16_SHIFTED)
         return set_error(SCLBM_E_INVALID_ARGUMENT, "the FP16 form uses the tile list (variant 2)");
+    if (variant == 5 && b->prec == SCLBM_FP64)
+        return set_error(SCLBM_E_INVALID_ARGUMENT, "the load-ahead tile list is for FP32/FP16 storage");
     b->use_units = variant == 3 || (variant == 0 && b->auto_units);
+    b->ahead = variant == 5;
     for (auto &g : b->graph)
         if (g) {
             cudaGraphExecDestroy(g);

@@ -332,10 +332,107 @@ template <typename S, typename T, int P> struct RingPops {
 // later iteration find them there.
 constexpr int PF_DIST = 2;
 
-template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS, bool PF = false>
+// Loads one row ahead (single pass): iteration r issues the loads of row r+1
+// into a third register buffer before it reduces row r (loaded during the
+// previous iteration) and collides row r-1, so a row's load latency overlaps a
+// whole iteration and each warp keeps two rows of loads in flight.  This is
+// what keeps the memory pipe full when part of a warp's lanes sit on solid
+// nodes and issue no loads.  Same arithmetic as fused2_tile, same results.
+template <typename S, typename T, int TX, int FLAGS>
+__device__ __forceinline__ void fused2_tile_ahead(const Fused2Args<S, T> &a, const int xb,
+                                                  const int yb, T (&s_rho)[2][4][TX],
+                                                  uint8_t (&s_m)[4][TX])
+{
+    constexpr bool SOLID = (FLAGS & KF_SOLID) != 0;
+    constexpr int W = TX - 2;
+    const int t = threadIdx.x;
+    const int nx = a.nx, ny = a.ny;
+    const int ncol = min(W, nx - xb);
+    const int nrow = min(a.tile_y, ny - yb);
+    const bool active = t <= ncol + 1;
+    const bool interior = t >= 1 && t <= ncol;
+    const int x = wrap1(xb - 1 + t, nx);
+    const int xl = wrap1(x - 1, nx), xr = wrap1(x + 1, nx);
+    auto node_of = [&](int r) { return (uint32_t)wrap1(yb + r, ny) * (uint32_t)nx + (uint32_t)x; };
+
+    // populations of row r into buf (solid nodes hold zeros on the domain path)
+    auto load_row = [&](int r, uint8_t m, T(&buf)[2][9]) {
+        if (active && (!SOLID || m || !a.solids_zero)) {
+            const uint32_t node = node_of(r);
+#pragma unroll
+            for (int k = 0; k < 2; ++k)
+#pragma unroll
+                for (int i = 0; i < 9; ++i)
+                    buf[k][i] = T(Store<S>::ld(a.fin[k] + (size_t)i * a.N + node));
+        }
+    };
+
+    // masks of rows r (mr) and r+1 (mr1) at iteration r; row r+2's is loaded there
+    uint8_t mr = 1, mr1 = 1;
+    if (SOLID && active) {
+        mr = a.mask[node_of(-1)];
+        mr1 = a.mask[node_of(0)];
+    }
+
+    T A[2][9], B[2][9], C[2][9];
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+#pragma unroll
+        for (int i = 0; i < 9; ++i) A[k][i] = B[k][i] = C[k][i] = T(0);
+    load_row(-1, mr, B);
+
+    // iteration r: load row r+1 into L, reduce row r (D), collide row r-1 (P)
+    auto body = [&](const int r, T(&L)[2][9], const T(&D)[2][9], const T(&P)[2][9]) {
+        uint8_t mr2 = 1;
+        if (SOLID && active && r + 2 <= nrow) mr2 = a.mask[node_of(r + 2)];
+        if (r + 1 <= nrow) load_row(r + 1, mr1, L);
+        T rho[2] = {T(0), T(0)};
+        uint8_t m = 0;
+        if (active) {
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                T s = T(0); // 0.0 + f0 + ... + f8, src/fluid.cpp:177-181
+#pragma unroll
+                for (int i = 0; i < 9; ++i) s += D[k][i];
+                rho[k] = s;
+            }
+            m = SOLID ? mr : 1;
+            if (SOLID && !m) rho[0] = rho[1] = T(0);
+        }
+        const int slot = (r + 1) & 3;
+        s_rho[0][slot][t] = rho[0];
+        s_rho[1][slot][t] = rho[1];
+        s_m[slot][t] = m;
+        __syncthreads();
+        if (r >= 1 && interior) {
+            const int sc = r & 3, sm = (r - 1) & 3, sp = (r + 1) & 3;
+            const int yc = wrap1(yb + r - 1, ny);
+            const Stencil<T> st{{s_rho[0][sm], s_rho[0][sc], s_rho[0][sp]},
+                                {s_rho[1][sm], s_rho[1][sc], s_rho[1][sp]},
+                                {s_m[sm], s_m[sc], s_m[sp]}, t};
+            const Nbr n = make_nbr(nx, x, xl, xr, yc, wrap1(yc - 1, ny), wrap1(yc + 1, ny));
+            collide_push<S, T, FLAGS>(a, P, st, n);
+        }
+        mr = mr1;
+        mr1 = mr2;
+    };
+    // three rows per trip: the buffers rotate roles (L, D, P) instead of copying
+    for (int r = -1; r <= nrow; r += 3) {
+        body(r, A, B, C);
+        if (r + 1 <= nrow) body(r + 1, C, A, B);
+        if (r + 2 <= nrow) body(r + 2, B, C, A);
+    }
+}
+
+template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS, bool PF = false,
+          bool AHEAD = false>
 __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int xb, const int yb,
                                             T (&s_rho)[2][4][TX], uint8_t (&s_m)[4][TX])
 {
+    if constexpr (AHEAD && !TWO_PASS) {
+        fused2_tile_ahead<S, T, TX, FLAGS>(a, xb, yb, s_rho, s_m);
+        return;
+    }
     constexpr bool SOLID = (FLAGS & KF_SOLID) != 0;
     constexpr int W = TX - 2;
     const int t = threadIdx.x;
@@ -431,15 +528,23 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
     }
 }
 
-// FP32 arithmetic: capped at 80 registers so six 128-thread CTAs are resident
-// per SM (the solid and force paths fit without spilling)
-template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS, bool PF = false>
-__global__ void __launch_bounds__(TX, sizeof(T) == 8 ? 1 : 6) k_fused2(const __grid_constant__ Fused2Args<S, T> a)
+// resident 128-thread CTAs per SM the register cap aims at: FP32 arithmetic
+// fits 80 registers (six CTAs) with two row buffers and 102 (five) with the
+// third buffer of the load-ahead form; FP64 is left uncapped
+template <typename T, bool AHEAD> constexpr int fused_min_ctas()
+{
+    return sizeof(T) == 8 ? 1 : (AHEAD ? 5 : 6);
+}
+
+template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS, bool PF = false,
+          bool AHEAD = false>
+__global__ void __launch_bounds__(TX, (fused_min_ctas<T, AHEAD>()))
+    k_fused2(const __grid_constant__ Fused2Args<S, T> a)
 {
     __shared__ T s_rho[2][4][TX];
     __shared__ uint8_t s_m[4][TX];
-    fused2_tile<S, T, TX, TWO_PASS, FLAGS, PF>(a, blockIdx.x * (TX - 2), blockIdx.y * a.tile_y,
-                                               s_rho, s_m);
+    fused2_tile<S, T, TX, TWO_PASS, FLAGS, PF, AHEAD>(a, blockIdx.x * (TX - 2),
+                                                      blockIdx.y * a.tile_y, s_rho, s_m);
 }
 
 // ---------------------------------------------------------------------------
@@ -547,29 +652,30 @@ template <typename S, typename T> inline int kernel_flags(const Fused2Args<S, T>
     return (a.c[0].force_on || a.c[1].force_on ? KF_FORCE : 0) | (a.has_solid ? KF_SOLID : 0);
 }
 
-template <typename S, typename T, int TX, bool TWO, int FLAGS, bool PF = false>
+template <typename S, typename T, int TX, bool TWO, int FLAGS, bool PF = false, bool AHEAD = false>
 inline cudaError_t launch_fused2_f(const Fused2Args<S, T> &a, cudaStream_t s)
 {
     constexpr int W = TX - 2;
     const dim3 grid((a.nx + W - 1) / W, (a.ny + a.tile_y - 1) / a.tile_y);
-    k_fused2<S, T, TX, TWO, FLAGS, PF><<<grid, TX, 0, s>>>(a);
+    k_fused2<S, T, TX, TWO, FLAGS, PF, AHEAD><<<grid, TX, 0, s>>>(a);
     return cudaGetLastError();
 }
 
-template <typename S, typename T, int TX, bool PF = false>
+template <typename S, typename T, int TX, bool PF = false, bool AHEAD = false>
 inline cudaError_t launch_fused2_tx(const Fused2Args<S, T> &a, bool two_pass, cudaStream_t s)
 {
     if (two_pass) return launch_fused2_f<S, T, TX, true, KF_FORCE | KF_SOLID>(a, s);
     switch (kernel_flags(a)) {
-    case 0: return launch_fused2_f<S, T, TX, false, 0, PF>(a, s);
-    case KF_FORCE: return launch_fused2_f<S, T, TX, false, KF_FORCE, PF>(a, s);
-    case KF_SOLID: return launch_fused2_f<S, T, TX, false, KF_SOLID, PF>(a, s);
-    default: return launch_fused2_f<S, T, TX, false, KF_FORCE | KF_SOLID, PF>(a, s);
+    case 0: return launch_fused2_f<S, T, TX, false, 0, PF, AHEAD>(a, s);
+    case KF_FORCE: return launch_fused2_f<S, T, TX, false, KF_FORCE, PF, AHEAD>(a, s);
+    case KF_SOLID: return launch_fused2_f<S, T, TX, false, KF_SOLID, PF, AHEAD>(a, s);
+    default: return launch_fused2_f<S, T, TX, false, KF_FORCE | KF_SOLID, PF, AHEAD>(a, s);
     }
 }
 
 // variant 1: two pass; 4: single pass with L2 row prefetch (128 threads);
-// otherwise the single-pass register tile
+// 5: single pass with loads one row ahead (128 threads); otherwise the
+// single-pass register tile
 template <typename S, typename T>
 inline cudaError_t launch_fused2_any(const Fused2Args<S, T> &a, int variant, int tx,
                                      cudaStream_t s)
@@ -578,6 +684,7 @@ inline cudaError_t launch_fused2_any(const Fused2Args<S, T> &a, int variant, int
     const bool two = variant == 1;
     if (tx == 64) return launch_fused2_tx<S, T, 64>(a, two, s);
     if (variant == 4) return launch_fused2_tx<S, T, 128, true>(a, false, s);
+    if (variant == 5) return launch_fused2_tx<S, T, 128, false, true>(a, false, s);
     return launch_fused2_tx<S, T, 128>(a, two, s);
 }
 

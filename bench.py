@@ -285,9 +285,24 @@ def run_ensemble(torch, sc, stream, steps, warmup, single_mlups, n=512):
     mlups = nodes / (ms * 1e-3) / 1e6
     fluid = sum(int(np.count_nonzero(m["mask"])) for m in members)
     del b, doms
+    # one large porous domain of the same geometry class (disks of radius 2-8 at
+    # the ensemble's mean fluid fraction), same storage, same timing
+    from sc_lbm_b200.validation import _porous_single
+    P, phi = _porous_single(sc, W, 4096, 4096, fluid / nodes, sc.FP32_SHIFTED)
+    P.step(warmup)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    P.step(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    porous_mlups = 4096 * 4096 / (e0.elapsed_time(e1) / steps * 1e-3) / 1e6
+    del P
     return {"value": round(mlups, 2), "unit": "MLUPS", "ms_per_step": round(ms, 5),
             "domains": n, "nodes": nodes, "fluid_fraction": round(fluid / nodes, 4),
             "efficiency_vs_single_4096": round(mlups / single_mlups, 4),
+            "single_porous_4096_mlups": round(porous_mlups, 2),
+            "single_porous_fluid_fraction": round(phi, 4),
+            "efficiency_vs_single_porous_4096": round(mlups / porous_mlups, 4),
             "tiles": ntiles, "ctas": grid, "precision": "fp32_shifted", "setup_s": round(setup_s, 1),
             "workload": f"{n} seeded porous two-component domains, Nx 64..512 x Ny 64..256 "
                         "(multiples of 16), porosity 0.5-0.9, G 0.8-1.2, Gs -0.3..0.3, "

@@ -193,6 +193,17 @@ def drainage(args):
     return out
 
 
+def _porous_single(sc, W, nx, ny, porosity, prec):
+    """One large seeded porous domain shaped like the ensemble members (disks
+    of radius 2-8, per-node noise), for the batch-efficiency comparison."""
+    m, _, phi = W.disk_mask(nx, ny, porosity, 2, 8, 31337, max_tries=400000, max_misses=2000)
+    d = sc.Domain(nx, ny, m, sc.make_params(ncomp=2, tau=(1.0, 1.0), g_fluid=(1.0, 1.0),
+                                            g_solid=(0.1, -0.1), rho_ref=(1.0, 1.0)), prec)
+    d.init_noise(0, 1.0, 0.01, 101)
+    d.init_noise(1, 1.0, 0.01, 102)
+    return d, phi
+
+
 def ensemble(args):
     torch, sc, W, stream = _env()
     n = 128 if args.quick else 512
@@ -200,37 +211,70 @@ def ensemble(args):
     t0 = time.time()
     members = W.ensemble(n)
     gen_s = time.time() - t0
-    doms = []
-    for m in members:
-        d = sc.Domain(m["nx"], m["ny"], m["mask"], W.params_of(m, sc), sc.FP32_SHIFTED)
-        d.upload_f(0, m["f1"])
-        d.upload_f(1, m["f2"])
-        doms.append(d)
-    nodes = sum(d.N for d in doms)
-    m0 = [d.mass_momentum() for d in doms]
-    b = sc.Batch(doms)  # tuned tile shapes per size class
-    ntiles, grid = b.info()
-    b.step(20)
-    ms = _timed(torch, stream, lambda: b.step(steps))
-    mlups = nodes * (steps) / (ms * 1e-3) / 1e6
-    drift = []
-    for d, a in zip(doms, m0):
-        m1 = d.mass_momentum()
-        drift.append(max(abs((m1[3 * c] - a[3 * c]) / a[3 * c]) for c in range(2)))
-    # one large domain of the same storage for the efficiency ratio
+    out = {"config": f"ensemble of {n} seeded porous domains, one batch per precision",
+           "steps": steps, "porosity_mean": float(np.mean([m["porosity"] for m in members])),
+           "generation_s": round(gen_s, 1)}
+    rho, finite = {}, {}
+    for prec, name in ((sc.FP32_SHIFTED, "fp32s"), (sc.FP64, "fp64")):
+        doms = []
+        for m in members:
+            d = sc.Domain(m["nx"], m["ny"], m["mask"], W.params_of(m, sc), prec)
+            d.upload_f(0, m["f1"])
+            d.upload_f(1, m["f2"])
+            doms.append(d)
+        nodes = sum(d.N for d in doms)
+        m0 = [d.mass_momentum() for d in doms]
+        b = sc.Batch(doms)  # tuned tile shapes per size class
+        ntiles, grid = b.info()
+        b.step(20)
+        ms = _timed(torch, stream, lambda: b.step(steps))
+        drift, ok = [], []
+        for d, a in zip(doms, m0):
+            try:
+                m1 = d.mass_momentum()
+                drift.append(max(abs((m1[3 * c] - a[3 * c]) / a[3 * c]) for c in range(2)))
+                ok.append(True)
+            except sc.capi.SclbmNonFinite:
+                ok.append(False)
+        finite[name] = ok
+        rho[name] = [d.download_rho(0) if good else None for d, good in zip(doms, ok)]
+        out[name] = {"mlups": round(nodes * steps / (ms * 1e-3) / 1e6, 1), "tiles": ntiles,
+                     "ctas": grid, "nodes": nodes, "non_finite_domains": int(len(ok) - sum(ok)),
+                     "max_mass_drift_finite": float(max(drift)) if drift else None}
+        del b, doms
+    bad = [k for k in range(n) if not finite["fp32s"][k] or not finite["fp64"][k]]
+    out["non_finite_params"] = [
+        {"k": k, "nx": members[k]["nx"], "ny": members[k]["ny"], "tau": members[k]["tau"][0],
+         "G": members[k]["G"], "Gs": members[k]["Gs"][0], "porosity": members[k]["porosity"],
+         "fp32s_finite": finite["fp32s"][k], "fp64_finite": finite["fp64"][k]} for k in bad[:20]]
+    errs = []
+    for k in range(n):
+        if finite["fp32s"][k] and finite["fp64"][k]:
+            fl = np.asarray(members[k]["mask"]).ravel() != 0
+            a, b_ = rho["fp32s"][k][fl], rho["fp64"][k][fl]
+            errs.append(float(np.max(np.abs(a - b_)) / np.mean(np.abs(b_))))
+    out["fp32s_rho1_max_over_mean_vs_fp64"] = {
+        "median": float(np.median(errs)), "max": float(np.max(errs))} if errs else None
+    # single large domains of the same storage for the efficiency ratio
     D = sc.Domain(4096, 4096, np.ones(4096 * 4096, np.int32),
                   sc.make_params(ncomp=2, g_fluid=(1.2, 1.2), rho_ref=(1.0, 1.0)), sc.FP32_SHIFTED)
     D.init_noise(0, 1.0, 0.01, 101)
     D.init_noise(1, 1.0, 0.01, 102)
     D.step(20)
     ms_big = _timed(torch, stream, lambda: D.step(200)) / 200
-    mlups_big = 4096 * 4096 / (ms_big * 1e-3) / 1e6
-    return {"config": f"ensemble of {n} domains, FP32-shifted, one batch (tile list {ntiles} tiles, "
-                      f"{grid} CTAs)", "steps": steps, "nodes": nodes,
-            "porosity_mean": float(np.mean([m["porosity"] for m in members])),
-            "mlups": round(mlups, 1), "single_4096_mlups": round(mlups_big, 1),
-            "efficiency_vs_single": round(mlups / mlups_big, 4),
-            "max_mass_drift": float(max(drift)), "generation_s": round(gen_s, 1)}
+    del D
+    P, phi = _porous_single(sc, W, 4096, 4096, out["porosity_mean"], sc.FP32_SHIFTED)
+    P.step(20)
+    ms_por = _timed(torch, stream, lambda: P.step(200)) / 200
+    del P
+    out["single_4096_all_fluid_mlups"] = round(4096 * 4096 / (ms_big * 1e-3) / 1e6, 1)
+    out["single_4096_porous_mlups"] = round(4096 * 4096 / (ms_por * 1e-3) / 1e6, 1)
+    out["single_4096_porosity"] = phi
+    out["efficiency_vs_single_all_fluid"] = round(out["fp32s"]["mlups"] /
+                                                  out["single_4096_all_fluid_mlups"], 4)
+    out["efficiency_vs_single_porous"] = round(out["fp32s"]["mlups"] /
+                                               out["single_4096_porous_mlups"], 4)
+    return out
 
 
 def spinodal(args):

@@ -43,6 +43,45 @@ def env_rank():
         int(os.environ.get("LOCAL_RANK", "0"))
 
 
+class Ranks:
+    """One process per GPU under torchrun: the barrier and the max over ranks
+    of device-timed values (NCCL on GPUs; gloo with device "cpu" in the CPU
+    tests).  World size 1 needs no process group."""
+
+    def __init__(self, backend="nccl", device="cuda"):
+        import datetime
+        import torch
+        import torch.distributed as dist
+        self.torch, self.dist, self.device = torch, dist, device
+        self.rank, self.world, self.local = env_rank()
+        self.owns_group = False
+        if self.world > 1 and not dist.is_initialized():
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+            self.owns_group = True
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+        if self.device == "cuda":
+            self.torch.cuda.synchronize()
+
+    def max(self, x: float) -> float:
+        if self.world == 1:
+            return x
+        t = self.torch.tensor([float(x)], dtype=self.torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def whole_job_mlups(self, nodes_per_rank: int, steps: int, ms_max: float) -> float:
+        """Lattice updates of all ranks over the slowest rank's time."""
+        return self.world * nodes_per_rank * steps / (ms_max * 1e-3) / 1e6
+
+    def close(self):
+        if self.owns_group:
+            self.dist.destroy_process_group()
+            self.owns_group = False
+
+
 def seeded_populations(nx, ny, seed):
     """f_i = rho/9 with rho = 1 +- 1% (the reference initialisers' rho/9 shape)."""
     from sc_lbm_b200.workloads import uniform
@@ -257,13 +296,15 @@ def time_domain(torch, sc, dom, stream, steps, warmup):
     return e0.elapsed_time(e1)
 
 
-def run_ensemble(torch, sc, stream, steps, warmup, single_mlups, n=512):
+def run_ensemble(torch, sc, stream, steps, warmup, single_mlups, ranks, n=512):
     """The uneven ensemble (512 seeded porous two-component domains, Nx in
     64..512, Ny in 64..256, per-domain G, Gs, tau) advanced by one batch:
-    one persistent launch per step from a CUDA graph, tuned tile shapes."""
+    one persistent launch per step from a CUDA graph, tuned tile shapes.
+    Each rank advances its own ensemble (weak scaling); times are the max over
+    ranks and the MLUPS count every rank's nodes."""
     from sc_lbm_b200 import workloads as W
     t0 = time.time()
-    members = W.ensemble(n)
+    members = W.ensemble(n, seed=2024 + ranks.rank)
     doms = []
     for m in members:
         d = sc.Domain(m["nx"], m["ny"], m["mask"], W.params_of(m, sc), sc.FP32_SHIFTED)
@@ -275,14 +316,14 @@ def run_ensemble(torch, sc, stream, steps, warmup, single_mlups, n=512):
     b = sc.Batch(doms)
     ntiles, grid = b.info()
     b.step(warmup)
-    torch.cuda.synchronize()
+    ranks.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     b.step(steps)
     e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
-    mlups = nodes / (ms * 1e-3) / 1e6
+    ranks.barrier()
+    ms = ranks.max(e0.elapsed_time(e1)) / steps
+    mlups = ranks.whole_job_mlups(nodes, 1, ms)
     fluid = sum(int(np.count_nonzero(m["mask"])) for m in members)
     del b, doms
     # one large porous domain of the same geometry class (disks of radius 2-8 at
@@ -290,12 +331,12 @@ def run_ensemble(torch, sc, stream, steps, warmup, single_mlups, n=512):
     from sc_lbm_b200.validation import _porous_single
     P, phi = _porous_single(sc, W, 4096, 4096, fluid / nodes, sc.FP32_SHIFTED)
     P.step(warmup)
-    torch.cuda.synchronize()
+    ranks.barrier()
     e0.record(stream)
     P.step(steps)
     e1.record(stream)
-    torch.cuda.synchronize()
-    porous_mlups = 4096 * 4096 / (e0.elapsed_time(e1) / steps * 1e-3) / 1e6
+    ranks.barrier()
+    porous_mlups = ranks.whole_job_mlups(4096 * 4096, 1, ranks.max(e0.elapsed_time(e1)) / steps)
     del P
     return {"value": round(mlups, 2), "unit": "MLUPS", "ms_per_step": round(ms, 5),
             "domains": n, "nodes": nodes, "fluid_fraction": round(fluid / nodes, 4),
@@ -311,13 +352,11 @@ def run_ensemble(torch, sc, stream, steps, warmup, single_mlups, n=512):
 
 def run_ours(args):
     import torch
-    import torch.distributed as dist
     import sc_lbm_b200 as sc
 
     rank, world, local = env_rank()
     torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    ranks = Ranks("nccl", "cuda")
     stream = torch.cuda.Stream()
     sc.set_stream(stream.cuda_stream)
 
@@ -328,17 +367,7 @@ def run_ours(args):
     params = sc.make_params(ncomp=2, tau=(1.0, 1.0), g_fluid=(G12, G12), g_solid=(0.0, 0.0),
                             rho_ref=(1.0, 1.0))
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     # --- FP32-shifted headline -------------------------------------------------
     d32 = sc.Domain(NX, NY, mask, params, sc.FP32_SHIFTED)
@@ -370,7 +399,7 @@ def run_ours(args):
     del d16
 
     ensemble = None if args.no_batch else run_ensemble(torch, sc, stream, args.steps, args.warmup,
-                                                       mlups32)
+                                                       mlups32, ranks)
 
     accuracy = accuracy_report(sc, mask, params, f1, f2) if rank == 0 else None
 
@@ -445,8 +474,7 @@ def run_ours(args):
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    ranks.close()
 
 
 def main():

@@ -37,6 +37,7 @@ struct sclbm_batch {
     int use_units = 1;
     int auto_units = 1; // tuned choice for variant 0
     int ahead = 0, grid_ahead = 0; // tile list with the load-ahead body (variant 5)
+    int flags = 0;                 // KF_FORCE / KF_SOLID if any domain needs them
     cudaGraphExec_t graph[2] = {nullptr, nullptr}; // by starting parity
     cudaStream_t graph_stream = nullptr;
 };
@@ -52,13 +53,15 @@ static cudaError_t batch_launch_any(sclbm_batch *b, int parity, cudaStream_t s)
     switch (b->prec) {
     case SCLBM_FP64:
         return launch_batch_fp64((const Fused2Args<double, double> *)b->d_args, b->d_tiles,
-                                 b->ntiles, parity, b->grid, s);
+                                 b->ntiles, parity, b->grid, b->flags, s);
     case SCLBM_FP32_SHIFTED:
         return launch_batch_f32((const Fused2Args<float, float> *)b->d_args, b->d_tiles,
-                                b->ntiles, parity, b->ahead ? b->grid_ahead : b->grid, b->ahead, s);
+                                b->ntiles, parity, b->ahead ? b->grid_ahead : b->grid, b->flags,
+                                b->ahead, s);
     default:
         return launch_batch_f16((const Fused2Args<__half, float> *)b->d_args, b->d_tiles,
-                                b->ntiles, parity, b->ahead ? b->grid_ahead : b->grid, b->ahead, s);
+                                b->ntiles, parity, b->ahead ? b->grid_ahead : b->grid, b->flags,
+                                b->ahead, s);
     }
 }
 
@@ -129,6 +132,8 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
             return set_error(SCLBM_E_INVALID_ARGUMENT,
                              "batch domains must be two-component, of one precision and in step");
         }
+        if (d->has_solid) b->flags |= KF_SOLID;
+        if (d->p.force_on[0] || d->p.force_on[1]) b->flags |= KF_FORCE;
         const SclbmTunedShape ts = tuned_shape(d->nx, d->ny, b->prec);
         ty[k] = tile_y_per_domain && tile_y_per_domain[k] > 0 ? tile_y_per_domain[k] : ts.tile_y;
         (ts.variant == 3 ? nodes_units : nodes_tiles) += (double)d->nx * (double)d->ny;

@@ -18,7 +18,7 @@ struct TileRef {
 // block of the current tile's domain is copied into shared memory, so the tile
 // body reads its fields from there instead of holding the whole block in
 // registers.
-template <typename S, typename T, bool AHEAD = false>
+template <typename S, typename T, int FLAGS = KF_FORCE | KF_SOLID, bool AHEAD = false>
 __global__ void __launch_bounds__(BATCH_TX, (fused_min_ctas<T, AHEAD>()))
     k_batch2(const Fused2Args<S, T> *__restrict__ doms, const TileRef *__restrict__ tiles,
              int ntiles, int parity)
@@ -38,36 +38,45 @@ __global__ void __launch_bounds__(BATCH_TX, (fused_min_ctas<T, AHEAD>()))
             __syncthreads();
             loaded = key;
         }
-        fused2_tile<S, T, BATCH_TX, false, KF_FORCE | KF_SOLID, false, AHEAD>(sa, tr.xb, tr.yb,
-                                                                            s_rho, s_m);
+        fused2_tile<S, T, BATCH_TX, false, FLAGS, false, AHEAD>(sa, tr.xb, tr.yb, s_rho, s_m);
         __syncthreads(); // the shared ring and block are reused by the next tile
     }
 }
 
+// flags: KF_FORCE / KF_SOLID when any domain of the batch has a volume force /
+// a solid node (the body drops what no domain needs)
 template <typename S, typename T, bool AHEAD = false>
 inline cudaError_t launch_batch_t(const Fused2Args<S, T> *doms, const TileRef *tiles, int ntiles,
-                                  int parity, int grid, cudaStream_t s)
+                                  int parity, int grid, int flags, cudaStream_t s)
 {
-    k_batch2<S, T, AHEAD><<<grid, BATCH_TX, 0, s>>>(doms, tiles, ntiles, parity);
+    if (AHEAD || flags == (KF_FORCE | KF_SOLID))
+        k_batch2<S, T, KF_FORCE | KF_SOLID, AHEAD><<<grid, BATCH_TX, 0, s>>>(doms, tiles, ntiles, parity);
+    else if (flags == KF_SOLID)
+        k_batch2<S, T, KF_SOLID><<<grid, BATCH_TX, 0, s>>>(doms, tiles, ntiles, parity);
+    else if (flags == KF_FORCE)
+        k_batch2<S, T, KF_FORCE><<<grid, BATCH_TX, 0, s>>>(doms, tiles, ntiles, parity);
+    else
+        k_batch2<S, T, 0><<<grid, BATCH_TX, 0, s>>>(doms, tiles, ntiles, parity);
     return cudaGetLastError();
 }
 
 template <typename S, typename T, bool AHEAD = false> inline int batch_blocks_per_sm_t()
 {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch2<S, T, AHEAD>, BATCH_TX, 0) !=
-        cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch2<S, T, KF_FORCE | KF_SOLID, AHEAD>,
+                                                      BATCH_TX, 0) != cudaSuccess)
         return 1;
     return n;
 }
 
 // `ahead` selects the load-ahead tile body (FP32 arithmetic only; ignored for FP64)
 cudaError_t launch_batch_fp64(const Fused2Args<double, double> *doms, const TileRef *tiles,
-                              int ntiles, int parity, int grid, cudaStream_t s);
+                              int ntiles, int parity, int grid, int flags, cudaStream_t s);
 cudaError_t launch_batch_f32(const Fused2Args<float, float> *doms, const TileRef *tiles,
-                             int ntiles, int parity, int grid, bool ahead, cudaStream_t s);
+                             int ntiles, int parity, int grid, int flags, bool ahead, cudaStream_t s);
 cudaError_t launch_batch_f16(const Fused2Args<__half, float> *doms, const TileRef *tiles,
-                             int ntiles, int parity, int grid, bool ahead, cudaStream_t s);
+                             int ntiles, int parity, int grid, int flags, bool ahead,
+                             cudaStream_t s);
 int batch_blocks_per_sm(sclbm_precision p, bool ahead = false);
 
 } // namespace sclbm

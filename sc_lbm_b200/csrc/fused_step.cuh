@@ -304,9 +304,8 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
                 const float fe = feq_dev(i, dr[k], r[k], ux, uy, usq15);
                 const T fi = f[k][i];
                 float v = fmaf(om, fe - fi, fi);
-                if constexpr (FORCE) {
-                    if (a.c[k].force_on) v += a.c[k].force[i];
-                }
+                // the force vector is zero for a component without a volume force
+                if constexpr (FORCE) v += a.c[k].force[i];
                 push_one<S, T, SOLID>(a, k, i, v, nf[i], n);
             }
         }

@@ -409,9 +409,9 @@ cudaError_t launch_density_fp64(const uint8_t *mask, const double *f0, const dou
 #include "batch_kernel.cuh"
 namespace sclbm {
 cudaError_t launch_batch_fp64(const Fused2Args<double, double> *doms, const TileRef *tiles,
-                              int ntiles, int parity, int grid, cudaStream_t s)
+                              int ntiles, int parity, int grid, int flags, cudaStream_t s)
 {
-    return launch_batch_t<double, double>(doms, tiles, ntiles, parity, grid, s);
+    return launch_batch_t<double, double>(doms, tiles, ntiles, parity, grid, flags, s);
 }
 int batch_blocks_per_sm_fp64() { return batch_blocks_per_sm_t<double, double>(); }
 } // namespace sclbm

@@ -44,16 +44,17 @@ cudaError_t launch_density_f16(const uint8_t *mask, const __half *f0, const __ha
 #include "batch_kernel.cuh"
 namespace sclbm {
 cudaError_t launch_batch_f32(const Fused2Args<float, float> *doms, const TileRef *tiles,
-                             int ntiles, int parity, int grid, bool ahead, cudaStream_t s)
+                             int ntiles, int parity, int grid, int flags, bool ahead, cudaStream_t s)
 {
-    if (ahead) return launch_batch_t<float, float, true>(doms, tiles, ntiles, parity, grid, s);
-    return launch_batch_t<float, float>(doms, tiles, ntiles, parity, grid, s);
+    if (ahead) return launch_batch_t<float, float, true>(doms, tiles, ntiles, parity, grid, flags, s);
+    return launch_batch_t<float, float>(doms, tiles, ntiles, parity, grid, flags, s);
 }
 cudaError_t launch_batch_f16(const Fused2Args<__half, float> *doms, const TileRef *tiles,
-                             int ntiles, int parity, int grid, bool ahead, cudaStream_t s)
+                             int ntiles, int parity, int grid, int flags, bool ahead,
+                             cudaStream_t s)
 {
-    if (ahead) return launch_batch_t<__half, float, true>(doms, tiles, ntiles, parity, grid, s);
-    return launch_batch_t<__half, float>(doms, tiles, ntiles, parity, grid, s);
+    if (ahead) return launch_batch_t<__half, float, true>(doms, tiles, ntiles, parity, grid, flags, s);
+    return launch_batch_t<__half, float>(doms, tiles, ntiles, parity, grid, flags, s);
 }
 int batch_blocks_per_sm_fp64();
 int batch_blocks_per_sm(sclbm_precision p, bool ahead)

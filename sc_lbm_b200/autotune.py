@@ -89,6 +89,30 @@ def accuracy(sc, W, member, steps):
     return out
 
 
+def select(results, margin):
+    """The shape to use from one precision's sweep: among the candidates within
+    `margin` (relative) of the fastest, the tile list with the most rows per
+    tile (fewest halo rows, which a mixed batch of small domains pays for more
+    than the homogeneous batch timed here), else the fastest."""
+    top = max(r["mlups"] for r in results)
+    near = [r for r in results if r["mlups"] >= (1.0 - margin) * top]
+    lists = [r for r in near if r["variant"] == 2]
+    pick = max(lists, key=lambda r: r["tile_y"]) if lists else max(near, key=lambda r: r["mlups"])
+    return {"variant": pick["variant"], "tile_y": pick["tile_y"], "mlups": pick["mlups"]}
+
+
+def reselect(path, margin):
+    """Re-apply the selection rule to a committed sweep (no GPU needed)."""
+    with open(path) as fh:
+        d = json.load(fh)
+    for c in d["classes"]:
+        for p in PREC_NAMES:
+            c["shapes"][p] = select(c["sweep"][p], margin)
+    d["margin"] = margin
+    with open(path, "w") as fh:
+        json.dump(d, fh, indent=1)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(HERE, "tuning", "b200.json"))
@@ -97,7 +121,15 @@ def main():
     ap.add_argument("--nodes", type=float, default=4e6, help="lattice nodes per timed batch")
     ap.add_argument("--accuracy-steps", type=int, default=100)
     ap.add_argument("--tolerance", type=float, default=1e-5)
+    ap.add_argument("--margin", type=float, default=0.03,
+                    help="shapes within this fraction of the fastest count as equal")
+    ap.add_argument("--reselect", action="store_true",
+                    help="re-apply the selection rule to the sweep in --out and exit")
     args = ap.parse_args()
+    if args.reselect:
+        reselect(args.out, args.margin)
+        print(f"re-selected {args.out}")
+        return
 
     import torch
     import sc_lbm_b200 as sc
@@ -126,9 +158,7 @@ def main():
                     res.append({"variant": variant, "tile_y": ty or 16, "mlups": round(mlups, 1),
                                 "ms_per_step": round(ms, 5)})
                 sweep[pname] = res
-                best = max(res, key=lambda r: r["mlups"])
-                shapes[pname] = {"variant": best["variant"], "tile_y": best["tile_y"],
-                                 "mlups": best["mlups"]}
+                shapes[pname] = select(res, args.margin)
                 del doms
             err = accuracy(sc, W, members[0], args.accuracy_steps)
             ok = [p for p in PREC_NAMES if err[p] <= args.tolerance]
@@ -143,7 +173,8 @@ def main():
     out = {"device": props.name, "sm_count": props.multi_processor_count,
            "command": "python -m sc_lbm_b200.autotune " + " ".join(sys.argv[1:]),
            "steps": args.steps, "warmup": args.warmup, "accuracy_steps": args.accuracy_steps,
-           "tolerance": args.tolerance, "seconds": round(time.time() - t_start, 1),
+           "tolerance": args.tolerance, "margin": args.margin,
+           "seconds": round(time.time() - t_start, 1),
            "note": "tile_y = rows (nodes per thread) per tile of the tile-list kernel; "
                    "variant 2 = tile list, 3 = strips x bands; mlups of a batch of "
                    "`domains` seeded porous domains of the representative size",

@@ -285,6 +285,33 @@ int sclbm_mass_momentum_noalloc(const void *f0, const void *f1, const uint8_t *m
 int sclbm_domain_run(sclbm_domain *d, const double *f1, const double *f2, int nsteps,
                      double *rho1, double *rho2);
 
+/* ------------------------------------------------------------------ output
+ * Files of a device lattice.  Text in the reference's format (Fluid::write_var
+ * through LbmIO::write_vector, src/fluid.cpp:303-353,
+ * include/io_operations/lbm_io.h:106-116): one line per lattice row, each
+ * value printed with 6 significant digits (%g) and followed by a space, rows
+ * cut exactly as write_var cuts them.  `what`: 0 density (write_density),
+ * 1 ux, 2 uy (write_ux / write_uy: momentum over density on fluid nodes),
+ * 3 populations into nine files <path>_<i>.txt (write_f).  Fluid::save_state
+ * (src/fluid.cpp:355-363) is what 0, 1 and 2 with "<name>_<step>.txt" paths.
+ * async = 1 queues the device-to-host copy on the library stream and returns;
+ * a worker thread formats and writes once the copy is done, while later steps
+ * run; sclbm_io_wait() joins all such writers and returns the first failure. */
+int sclbm_domain_write_text(sclbm_domain *d, int comp, int what, const char *path, int async);
+int sclbm_io_wait(void);
+/* Fluid::restart_from_file, src/fluid.cpp:285-298: populations from the nine
+ * text files <prefix>_<i>.txt (ny rows of nx values each), uploaded as comp. */
+int sclbm_domain_read_text_f(sclbm_domain *d, int comp, const char *prefix);
+/* Host-only: write nx*ny values as write_var does / read them back (no device). */
+int sclbm_write_rows(const char *path, const double *v, size_t nx, size_t ny);
+int sclbm_read_rows(const char *path, double *v, size_t nx, size_t ny);
+/* Exact binary checkpoint of the stored populations (any storage precision)
+ * with the mask and sizes; load requires a domain of the same size, component
+ * count, precision and mask, and continues the run bit for bit.  No reference
+ * counterpart (the reference restarts only from its 6-digit text files). */
+int sclbm_domain_checkpoint_save(sclbm_domain *d, const char *path);
+int sclbm_domain_checkpoint_load(sclbm_domain *d, const char *path);
+
 /* ------------------------------------------------------------------- batch
  * Many independent domains of one precision advanced together: one launch
  * per time step walks a tile list drawn from all domains, and the launch

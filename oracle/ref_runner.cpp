@@ -11,6 +11,7 @@
 //
 // usage: sclbm_ref_runner case <spec.txt>      (writes the path named by `out`)
 //        sclbm_ref_runner bench <nx> <ny> <steps> <seed>
+//        sclbm_ref_runner text <f.bin> <nx> <ny> <prefix>
 #include <chrono>
 #include <cstdint>
 #include <cstdio>
@@ -339,11 +340,31 @@ int run_bench(size_t nx, size_t ny, int steps, unsigned seed)
     return 0;
 }
 
+// The reference's own text output of one all-fluid component whose
+// populations are read from f.bin (9*nx*ny doubles): write_density,
+// write_ux, write_uy and write_f with the given path prefix
+// (src/fluid.cpp:303-353, include/fluid.h:219-251).
+int run_text(const std::string &fbin, size_t nx, size_t ny, const std::string &prefix)
+{
+    Geometry geom(nx, ny);
+    Fluid fl("fluid", 1. / 3, 1.0);
+    fl.simple_ini(geom, 1.0);
+    fl.get_f_dist() = read_doubles(fbin, 9 * nx * ny);
+    fl.write_density(prefix + "_rho.txt");
+    fl.write_ux(prefix + "_ux.txt", geom);
+    fl.write_uy(prefix + "_uy.txt", geom);
+    fl.write_f(prefix + "_f");
+    return 0;
+}
+
 } // namespace
 
 int main(int argc, char **argv)
 {
     if (argc >= 3 && std::string(argv[1]) == "case") return run_case(argv[2]);
+    if (argc >= 6 && std::string(argv[1]) == "text")
+        return run_text(argv[2], std::strtoull(argv[3], 0, 10), std::strtoull(argv[4], 0, 10),
+                        argv[5]);
     if (argc >= 5 && std::string(argv[1]) == "bench")
         return run_bench(std::strtoull(argv[2], 0, 10), std::strtoull(argv[3], 0, 10),
                          std::atoi(argv[4]), argc > 5 ? (unsigned)std::atoi(argv[5]) : 1u);

@@ -290,6 +290,31 @@ class Domain(_Handle):
     def device_bytes(self) -> int:
         return int(lib().sclbm_domain_device_bytes(self._h))
 
+    # reference-format text output (density 0, ux 1, uy 2, populations 3)
+    def write_text(self, comp, what, path, asynchronous=False):
+        call("sclbm_domain_write_text", self._h, int(comp), int(what), str(path).encode(),
+             1 if asynchronous else 0)
+
+    def write_density(self, comp, path, asynchronous=False):
+        self.write_text(comp, 0, path, asynchronous)
+
+    def save_state(self, comp, frho, fux, fuy, step, asynchronous=False):
+        """Fluid::save_state: <frho>_<step>.txt, <fux>_<step>.txt, <fuy>_<step>.txt"""
+        for what, name in ((0, frho), (1, fux), (2, fuy)):
+            self.write_text(comp, what, f"{name}_{int(step)}.txt", asynchronous)
+
+    def write_f(self, comp, prefix, asynchronous=False):
+        self.write_text(comp, 3, prefix, asynchronous)
+
+    def restart_from_file(self, comp, prefix):
+        call("sclbm_domain_read_text_f", self._h, int(comp), str(prefix).encode())
+
+    def checkpoint_save(self, path):
+        call("sclbm_domain_checkpoint_save", self._h, str(path).encode())
+
+    def checkpoint_load(self, path):
+        call("sclbm_domain_checkpoint_load", self._h, str(path).encode())
+
     def run(self, f1, f2, nsteps, rho1, rho2=None):
         call("sclbm_domain_run", self._h, _dp(f1), None if f2 is None else _dp(f2), int(nsteps),
              _dp(rho1), None if rho2 is None else _dp(rho2))
@@ -325,6 +350,24 @@ def tuned_config(nx: int, ny: int, precision: int | None = None) -> dict:
     call("sclbm_tuned_config", int(nx), int(ny), -1 if precision is None else int(precision),
          C.byref(t), C.byref(v), C.byref(r))
     return {"tile_y": t.value, "variant": v.value, "recommended_precision": r.value}
+
+
+def io_wait():
+    """Join the asynchronous text writers; raises the first failure."""
+    call("sclbm_io_wait")
+
+
+def write_rows(path, values, nx, ny):
+    v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+    if v.size != nx * ny:
+        raise ValueError("values must hold nx*ny entries")
+    call("sclbm_write_rows", str(path).encode(), _dp(v), int(nx), int(ny))
+
+
+def read_rows(path, nx, ny) -> np.ndarray:
+    out = np.empty(nx * ny)
+    call("sclbm_read_rows", str(path).encode(), _dp(out), int(nx), int(ny))
+    return out
 
 
 def synchronize():

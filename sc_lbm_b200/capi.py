@@ -124,6 +124,13 @@ SIGNATURES = {
     "sclbm_batch_step": (C.c_int, [_VP, C.c_int, C.c_int]),
     "sclbm_batch_set_kernel": (C.c_int, [_VP, C.c_int]),
     "sclbm_batch_info": (C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "sclbm_domain_write_text": (C.c_int, [_VP, C.c_int, C.c_int, C.c_char_p, C.c_int]),
+    "sclbm_io_wait": (C.c_int, []),
+    "sclbm_domain_read_text_f": (C.c_int, [_VP, C.c_int, C.c_char_p]),
+    "sclbm_write_rows": (C.c_int, [C.c_char_p, _D, _SZ, _SZ]),
+    "sclbm_read_rows": (C.c_int, [C.c_char_p, _D, _SZ, _SZ]),
+    "sclbm_domain_checkpoint_save": (C.c_int, [_VP, C.c_char_p]),
+    "sclbm_domain_checkpoint_load": (C.c_int, [_VP, C.c_char_p]),
     "sclbm_tuned_config": (C.c_int, [_SZ, _SZ, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                      C.POINTER(C.c_int)]),
 }

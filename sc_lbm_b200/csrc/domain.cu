@@ -569,6 +569,59 @@ static int rho_to_staging(sclbm_domain *d, int comp, cudaStream_t s)
     return SCLBM_OK;
 }
 
+} // extern "C"
+
+namespace sclbm {
+// One output field of component comp as FP64 values copied into host (pinned)
+// memory, queued on stream s and not synchronised: what = 0 density, 1 ux,
+// 2 uy (N values, Fluid::compute_density / compute_velocities), 3 the nine
+// population arrays (9N values, direction-major).  The staging buffer is
+// reused across directions; stream order keeps each copy before the next
+// conversion.
+int domain_field_async(sclbm_domain *d, int comp, int what, double *host, cudaStream_t s)
+{
+    const size_t N = d->N;
+    const int g = grid_for(N, 256);
+    const void *src = d->buf[d->parity][comp];
+    const double rr = d->p.rho_ref[comp];
+    if (what == 0) {
+        int rc = rho_to_staging(d, comp, s);
+        if (rc) return rc;
+        SCLBM_CUDA(cudaMemcpyAsync(host, d->staging, N * 8, cudaMemcpyDeviceToHost, s));
+        return SCLBM_OK;
+    }
+    if (what == 1 || what == 2) {
+        double *a = d->staging, *b = d->staging + N;
+        switch (d->prec) {
+        case SCLBM_FP64: k_velocity<double><<<g, 256, 0, s>>>(N, d->d_mask, (const double *)src, a, b, 0.0, 0); break;
+        case SCLBM_FP32_SHIFTED: k_velocity<float><<<g, 256, 0, s>>>(N, d->d_mask, (const float *)src, a, b, rr, 1); break;
+        default: k_velocity<__half><<<g, 256, 0, s>>>(N, d->d_mask, (const __half *)src, a, b, rr, 1); break;
+        }
+        SCLBM_LAUNCHED("velocity");
+        SCLBM_CUDA(cudaMemcpyAsync(host, what == 1 ? a : b, N * 8, cudaMemcpyDeviceToHost, s));
+        return SCLBM_OK;
+    }
+    for (int i = 0; i < 9; ++i) {
+        if (d->prec == SCLBM_FP64) {
+            SCLBM_CUDA(cudaMemcpyAsync(host + i * N, (const double *)src + i * N, N * 8,
+                                       cudaMemcpyDeviceToHost, s));
+            continue;
+        }
+        if (d->prec == SCLBM_FP32_SHIFTED)
+            k_download_dir<float><<<g, 256, 0, s>>>(N, d->d_mask, (const float *)src + i * N,
+                                                    d->staging, w_eq(i) * rr);
+        else
+            k_download_dir<__half><<<g, 256, 0, s>>>(N, d->d_mask, (const __half *)src + i * N,
+                                                     d->staging, w_eq(i) * rr);
+        SCLBM_LAUNCHED("download conversion");
+        SCLBM_CUDA(cudaMemcpyAsync(host + i * N, d->staging, N * 8, cudaMemcpyDeviceToHost, s));
+    }
+    return SCLBM_OK;
+}
+} // namespace sclbm
+
+extern "C" {
+
 int sclbm_domain_download_rho(sclbm_domain *d, int comp, double *rho, size_t count)
 {
     int rc = check_comp(d, comp, count, d ? d->N : 0);

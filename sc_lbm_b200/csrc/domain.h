@@ -25,6 +25,7 @@ namespace sclbm {
 size_t elem_size(sclbm_precision p);
 int domain_launch_step(sclbm_domain *d, cudaStream_t s);
 int domain_default_tile_y(const sclbm_domain *d);
+int domain_field_async(sclbm_domain *d, int comp, int what, double *host, cudaStream_t s);
 // fill the kernel argument blocks for the current parity
 void domain_fused2_args(const sclbm_domain *d, Fused2Args<double, double> *a64,
                         Fused2Args<float, float> *a32, Fused2Args<__half, float> *a16);

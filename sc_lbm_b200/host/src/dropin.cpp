@@ -331,15 +331,17 @@ void Fluid::restart_from_file(const std::string &fname)
     }
 }
 
-// rows of Nx values (src/fluid.cpp:307-343 writes nothing for a 1-node lattice)
+// rows of Nx values cut as src/fluid.cpp:303-343 cuts them (sclbm_write_rows)
 void Fluid::write_var(const std::vector<double> &variable, const std::string &fname) const
 {
-    std::vector<std::vector<double>> rows;
-    if (Nx * Ny > 1)
-        for (size_t y = 0; y < Ny; ++y)
-            rows.emplace_back(variable.begin() + y * Nx, variable.begin() + (y + 1) * Nx);
-    LbmIO io(fname, " ", true, {Ny, Nx, 0});
-    io.write_vector(rows);
+    if (variable.size() < Nx * Ny) throw std::out_of_range("vector::_M_range_check: short variable");
+    const int rc = sclbm_write_rows(fname.c_str(), variable.data(), Nx, Ny);
+    if (rc == SCLBM_E_RUNTIME) {
+        char buf[1024];
+        sclbm_last_error(buf, sizeof buf);
+        throw std::ios_base::failure(buf);
+    }
+    check(rc);
 }
 
 void Fluid::write_var(const std::vector<double> &variable, const std::string &fname, const bool) const

@@ -312,6 +312,28 @@ int sclbm_read_rows(const char *path, double *v, size_t nx, size_t ny);
 int sclbm_domain_checkpoint_save(sclbm_domain *d, const char *path);
 int sclbm_domain_checkpoint_load(sclbm_domain *d, const char *path);
 
+/* ---------------------------------------------------------------- analysis
+ * Measurements computed on the device from the stored populations (FP64
+ * densities and velocities as Fluid::compute_density / compute_velocities
+ * give them); deterministic reductions.  No reference counterpart in the
+ * library: they restate the reference's post-processing scripts. */
+/* Laplace law, compute_surface_tension.py:55-73: out[0] = p(x_in, y_in) -
+ * p(x_out, y_out) with p = (rho_b + rho_d)/3 + G rho_b rho_d / 3 (bulk
+ * component `bulk`, droplet the other); out[1] = radius = the mean of half the
+ * row extent (out[2]) and half the column extent (out[3]) of the nodes with
+ * rho_d < rho_b and rho_disp < rho_b <= rho_bulk; out[4] = their number. */
+int sclbm_domain_laplace_measure(sclbm_domain *d, int bulk, double G, double rho_bulk,
+                                 double rho_disp, size_t x_in, size_t y_in, size_t x_out,
+                                 size_t y_out, double out[5]);
+/* Over the fluid nodes of component comp: out[0] = max |u| (spurious
+ * currents, vel_mag of scripts/benchmark_utils.py:55-58), out[1] = mean of
+ * the nonzero |u| (ave, :60-63), out[2] = number of nonzero |u|. */
+int sclbm_domain_velocity_stats(sclbm_domain *d, int comp, double out[3]);
+/* Row profile: prof[y] = mean of u_x (axis 0) or u_y (axis 1) over the fluid
+ * nodes of row y (0 for a row without fluid); count must be ny.  The channel
+ * profile compared with scripts/benchmark_utils.py:8-52. */
+int sclbm_domain_profile(sclbm_domain *d, int comp, int axis, double *prof, size_t count);
+
 /* ------------------------------------------------------------------- batch
  * Many independent domains of one precision advanced together: one launch
  * per time step walks a tile list drawn from all domains, and the launch

@@ -315,6 +315,24 @@ class Domain(_Handle):
     def checkpoint_load(self, path):
         call("sclbm_domain_checkpoint_load", self._h, str(path).encode())
 
+    # measurements on the device (the reference's post-processing scripts)
+    def laplace_measure(self, bulk, G, rho_bulk, rho_disp, p_in, p_out) -> dict:
+        out = np.zeros(5)
+        call("sclbm_domain_laplace_measure", self._h, int(bulk), float(G), float(rho_bulk),
+             float(rho_disp), int(p_in[0]), int(p_in[1]), int(p_out[0]), int(p_out[1]), _dp(out))
+        return {"dp": out[0], "R": out[1], "R_rows": out[2], "R_cols": out[3],
+                "band_nodes": int(out[4])}
+
+    def velocity_stats(self, comp) -> dict:
+        out = np.zeros(3)
+        call("sclbm_domain_velocity_stats", self._h, int(comp), _dp(out))
+        return {"max_u": out[0], "mean_nonzero_u": out[1], "nonzero": int(out[2])}
+
+    def profile(self, comp, axis=0) -> np.ndarray:
+        out = np.zeros(self.ny)
+        call("sclbm_domain_profile", self._h, int(comp), int(axis), _dp(out), self.ny)
+        return out
+
     def run(self, f1, f2, nsteps, rho1, rho2=None):
         call("sclbm_domain_run", self._h, _dp(f1), None if f2 is None else _dp(f2), int(nsteps),
              _dp(rho1), None if rho2 is None else _dp(rho2))

@@ -131,6 +131,10 @@ SIGNATURES = {
     "sclbm_read_rows": (C.c_int, [C.c_char_p, _D, _SZ, _SZ]),
     "sclbm_domain_checkpoint_save": (C.c_int, [_VP, C.c_char_p]),
     "sclbm_domain_checkpoint_load": (C.c_int, [_VP, C.c_char_p]),
+    "sclbm_domain_laplace_measure": (C.c_int, [_VP, C.c_int, C.c_double, C.c_double, C.c_double,
+                                               _SZ, _SZ, _SZ, _SZ, _D]),
+    "sclbm_domain_velocity_stats": (C.c_int, [_VP, C.c_int, _D]),
+    "sclbm_domain_profile": (C.c_int, [_VP, C.c_int, C.c_int, _D, _SZ]),
     "sclbm_tuned_config": (C.c_int, [_SZ, _SZ, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                      C.POINTER(C.c_int)]),
 }

@@ -38,7 +38,9 @@ __global__ void __launch_bounds__(BATCH_TX, (fused_min_ctas<T, AHEAD>()))
             __syncthreads();
             loaded = key;
         }
-        fused2_tile<S, T, BATCH_TX, false, FLAGS, false, AHEAD>(sa, tr.xb, tr.yb, s_rho, s_m);
+        // alternate march directions of a domain's row bands (see fused2_tile)
+        fused2_tile<S, T, BATCH_TX, false, FLAGS, false, AHEAD>(sa, tr.xb, tr.yb, s_rho, s_m,
+                                                                ((tr.yb / sa.tile_y) & 1) != 0);
         __syncthreads(); // the shared ring and block are reused by the next tile
     }
 }

@@ -423,10 +423,18 @@ __device__ __forceinline__ void fused2_tile_ahead(const Fused2Args<S, T> &a, con
     }
 }
 
+// Tiles march up their rows (down = false) or down them (down = true).  The
+// launches give vertically neighbouring tiles opposite directions, so the two
+// rows a pair of tiles both read (each one's halo row is the other's edge row)
+// are read by both near the same time -- at both tiles' starts or at both
+// ends -- and the second read finds them in L2 instead of going to DRAM.
+// Direction changes only the order of the rows; every node gets the same
+// arithmetic and every destination slot the same single write.
 template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS, bool PF = false,
           bool AHEAD = false>
 __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int xb, const int yb,
-                                            T (&s_rho)[2][4][TX], uint8_t (&s_m)[4][TX])
+                                            T (&s_rho)[2][4][TX], uint8_t (&s_m)[4][TX],
+                                            const bool down = false)
 {
     if constexpr (AHEAD && !TWO_PASS) {
         fused2_tile_ahead<S, T, TX, FLAGS>(a, xb, yb, s_rho, s_m);
@@ -442,21 +450,27 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
     const bool interior = t >= 1 && t <= ncol;
     const int x = wrap1(xb - 1 + t, nx);
     const int xl = wrap1(x - 1, nx), xr = wrap1(x + 1, nx);
+    // row of the tile (-1 .. nrow, halos included) visited in iteration q
+    auto phys = [&](int q) { return down ? nrow - 1 - q : q; };
 
     // the mask of the next row is loaded one iteration ahead, so the population
     // loads of a row never wait on its mask load
     uint8_t m_ahead = 1;
-    if (SOLID && active) m_ahead = a.mask[(uint32_t)wrap1(yb - 1, ny) * (uint32_t)nx + (uint32_t)x];
+    if (SOLID && active)
+        m_ahead = a.mask[(uint32_t)wrap1(yb + phys(-1), ny) * (uint32_t)nx + (uint32_t)x];
 
-    // one row: load row r into cur, publish its density, collide row r-1 (prev)
-    auto row = [&](const int r, T(&cur)[2][9], const T(&prev)[2][9]) {
+    // iteration q: load row phys(q) into cur, publish its density, collide row
+    // phys(q-1) (prev) from the densities of rows phys(q-2), phys(q-1), phys(q)
+    auto row = [&](const int q, T(&cur)[2][9], const T(&prev)[2][9]) {
+        const int r = phys(q);
         const int y = wrap1(yb + r, ny);
-        const int slot = (r + 1) & 3;
+        const int slot = (q + 1) & 3;
         if constexpr (PF) {
-            const int rp = r + PF_DIST;
-            if (t < 18 && rp <= nrow) {
+            const int qp = q + PF_DIST;
+            if (t < 18 && qp <= nrow) {
                 const int k = t >= 9 ? 1 : 0, i = t - 9 * k;
-                const S *arr = a.fin[k] + (size_t)i * a.N + (size_t)wrap1(yb + rp, ny) * (size_t)nx;
+                const S *arr =
+                    a.fin[k] + (size_t)i * a.N + (size_t)wrap1(yb + phys(qp), ny) * (size_t)nx;
                 const uintptr_t lo = (uintptr_t)(arr + max(xb - 1, 0)) & ~uintptr_t(15);
                 const uintptr_t end = (uintptr_t)(a.fin[k] + 9 * a.N) & ~uintptr_t(15);
                 const uintptr_t up = ((uintptr_t)(arr + min(xb + ncol + 1, nx)) + 15) & ~uintptr_t(15);
@@ -470,8 +484,8 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
             const uint32_t node = (uint32_t)y * (uint32_t)nx + (uint32_t)x;
             if (SOLID) {
                 m = m_ahead;
-                if (r < nrow)
-                    m_ahead = a.mask[(uint32_t)wrap1(yb + r + 1, ny) * (uint32_t)nx + (uint32_t)x];
+                if (q < nrow)
+                    m_ahead = a.mask[(uint32_t)wrap1(yb + phys(q + 1), ny) * (uint32_t)nx + (uint32_t)x];
             }
             // solid nodes hold zeros on the domain path: nothing to read there
             const bool need_pops = (!TWO_PASS || (interior && r >= 0 && r < nrow)) &&
@@ -504,12 +518,14 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
         s_m[slot][t] = m;
         __syncthreads();
 
-        if (r >= 1 && interior) {
-            const int sc = r & 3, sm = (r - 1) & 3, sp = (r + 1) & 3;
-            const int yc = wrap1(yb + r - 1, ny);
-            const Stencil<T> st{{s_rho[0][sm], s_rho[0][sc], s_rho[0][sp]},
-                                {s_rho[1][sm], s_rho[1][sc], s_rho[1][sp]},
-                                {s_m[sm], s_m[sc], s_m[sp]}, t};
+        if (q >= 1 && interior) {
+            // slots of the rows below (sb), at (sc) and above (sa) the node
+            const int s_old = (q - 1) & 3, sc = q & 3, s_new = (q + 1) & 3;
+            const int sb = down ? s_new : s_old, sa = down ? s_old : s_new;
+            const int yc = wrap1(yb + phys(q - 1), ny);
+            const Stencil<T> st{{s_rho[0][sb], s_rho[0][sc], s_rho[0][sa]},
+                                {s_rho[1][sb], s_rho[1][sc], s_rho[1][sa]},
+                                {s_m[sb], s_m[sc], s_m[sa]}, t};
             const Nbr n = make_nbr(nx, x, xl, xr, yc, wrap1(yc - 1, ny), wrap1(yc + 1, ny));
             collide_push<S, T, FLAGS>(a, prev, st, n);
         }
@@ -521,9 +537,9 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
 #pragma unroll
         for (int i = 0; i < 9; ++i) A[k][i] = B[k][i] = T(0);
     // two rows per trip so the buffers swap roles instead of being copied
-    for (int r = -1; r <= nrow; r += 2) {
-        row(r, A, B);
-        if (r + 1 <= nrow) row(r + 1, B, A);
+    for (int q = -1; q <= nrow; q += 2) {
+        row(q, A, B);
+        if (q + 1 <= nrow) row(q + 1, B, A);
     }
 }
 
@@ -543,7 +559,8 @@ __global__ void __launch_bounds__(TX, (fused_min_ctas<T, AHEAD>()))
     __shared__ T s_rho[2][4][TX];
     __shared__ uint8_t s_m[4][TX];
     fused2_tile<S, T, TX, TWO_PASS, FLAGS, PF, AHEAD>(a, blockIdx.x * (TX - 2),
-                                                      blockIdx.y * a.tile_y, s_rho, s_m);
+                                                      blockIdx.y * a.tile_y, s_rho, s_m,
+                                                      (blockIdx.y & 1) != 0);
 }
 
 // ---------------------------------------------------------------------------

@@ -253,8 +253,11 @@ int sclbm_domain_mass_momentum(sclbm_domain *d, double out[7]);
  *   4 = variant 2 with the row segments of each tile prefetched into L2 two
  *       rows ahead (cp.async.bulk.prefetch), 128 threads per tile;
  *   5 = variant 2 with the loads of row r+1 issued before row r is reduced
- *       (a third row buffer in registers), 128 threads per tile.
- * tile_y = rows per tile of variants 1, 2, 4 and 5 (0 keeps the default). */
+ *       (a third row buffer in registers), 128 threads per tile;
+ *   6 = variant 2 with each row's collision done by consecutive threads on
+ *       its fluid nodes only (populations staged in shared memory), for
+ *       lattices with solid nodes (all-fluid lattices run variant 2).
+ * tile_y = rows per tile of variants 1, 2, 4, 5 and 6 (0 keeps the default). */
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y);
 /* Threads per tile of the register-tile kernel (variants 1, 2): 64 or 128. */
 int sclbm_domain_set_threads(sclbm_domain *d, int tx);
@@ -349,7 +352,8 @@ void sclbm_batch_destroy(sclbm_batch *b);
  * variant of the size class holding most of the batch's nodes); 2 = tile
  * list, tile_y rows per tile, register-tile body; 3 = 128-column strips x
  * row bands of one common height, pipelined body (FP64 and FP32 storage);
- * 5 = tile list with the load-ahead body (FP32 and FP16 storage). */
+ * 5 = tile list with the load-ahead body, 6 = tile list with the compacted
+ * fluid-lane body (FP32 and FP16 storage). */
 int sclbm_batch_set_kernel(sclbm_batch *b, int variant);
 /* advance every domain nsteps; use_graph = 1 replays a captured CUDA graph */
 int sclbm_batch_step(sclbm_batch *b, int nsteps, int use_graph);

@@ -36,7 +36,8 @@ struct sclbm_batch {
     int ntiles = 0, grid = 0, parity = 0;
     int use_units = 1;
     int auto_units = 1; // tuned choice for variant 0
-    int ahead = 0, grid_ahead = 0; // tile list with the load-ahead body (variant 5)
+    int body = BODY_TILE;          // tile-list body: 2 register tile, 5 load ahead, 6 compacted
+    int grid_body[3] = {0, 0, 0};  // resident grid of each body
     int flags = 0;                 // KF_FORCE / KF_SOLID if any domain needs them
     cudaGraphExec_t graph[2] = {nullptr, nullptr}; // by starting parity
     cudaStream_t graph_stream = nullptr;
@@ -56,12 +57,10 @@ static cudaError_t batch_launch_any(sclbm_batch *b, int parity, cudaStream_t s)
                                  b->ntiles, parity, b->grid, b->flags, s);
     case SCLBM_FP32_SHIFTED:
         return launch_batch_f32((const Fused2Args<float, float> *)b->d_args, b->d_tiles,
-                                b->ntiles, parity, b->ahead ? b->grid_ahead : b->grid, b->flags,
-                                b->ahead, s);
+                                b->ntiles, parity, b->grid_body[b->body], b->flags, b->body, s);
     default:
         return launch_batch_f16((const Fused2Args<__half, float> *)b->d_args, b->d_tiles,
-                                b->ntiles, parity, b->ahead ? b->grid_ahead : b->grid, b->flags,
-                                b->ahead, s);
+                                b->ntiles, parity, b->grid_body[b->body], b->flags, b->body, s);
     }
 }
 
@@ -153,9 +152,9 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
     int per_sm = batch_blocks_per_sm(b->prec);
     if (per_sm < 1) per_sm = 1;
     b->grid = std::max(1, std::min(b->ntiles, per_sm * sm_count()));
-    if (b->prec != SCLBM_FP64) {
-        const int pa = std::max(1, batch_blocks_per_sm(b->prec, true));
-        b->grid_ahead = std::max(1, std::min(b->ntiles, pa * sm_count()));
+    for (int body = 0; body < 3; ++body) {
+        const int pb = b->prec == SCLBM_FP64 ? per_sm : std::max(1, batch_blocks_per_sm(b->prec, body));
+        b->grid_body[body] = std::max(1, std::min(b->ntiles, pb * sm_count()));
     }
     switch (b->prec) {
     case SCLBM_FP64: rc = upload_args<double, double>(b, ty); break;
@@ -214,14 +213,15 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
 int sclbm_batch_set_kernel(sclbm_batch *b, int variant)
 {
     if (!b) return set_error(SCLBM_E_INVALID_ARGUMENT, "null batch");
-    if (variant != 0 && variant != 2 && variant != 3 && variant != 5)
-        return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0, 2, 3 or 5");
+    if (variant != 0 && variant != 2 && variant != 3 && variant != 5 && variant != 6)
+        return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0, 2, 3, 5 or 6");
     if (variant == 3 && b->prec == SCLBM_FP16_SHIFTED)
         return set_error(SCLBM_E_INVALID_ARGUMENT, "the FP16 form uses the tile list (variant 2)");
-    if (variant == 5 && b->prec == SCLBM_FP64)
-        return set_error(SCLBM_E_INVALID_ARGUMENT, "the load-ahead tile list is for FP32/FP16 storage");
+    if ((variant == 5 || variant == 6) && b->prec == SCLBM_FP64)
+        return set_error(SCLBM_E_INVALID_ARGUMENT,
+                         "the load-ahead and compacted tile lists are for FP32/FP16 storage");
     b->use_units = variant == 3 || (variant == 0 && b->auto_units);
-    b->ahead = variant == 5;
+    b->body = variant == 5 ? BODY_AHEAD : (variant == 6 ? BODY_COMPACT : BODY_TILE);
     for (auto &g : b->graph)
         if (g) {
             cudaGraphExecDestroy(g);
@@ -234,7 +234,8 @@ int sclbm_batch_info(const sclbm_batch *b, int *ntiles, int *grid_ctas)
 {
     if (!b) return set_error(SCLBM_E_INVALID_ARGUMENT, "null batch");
     if (ntiles) *ntiles = b->ntiles;
-    if (grid_ctas) *grid_ctas = b->grid;
+    if (grid_ctas)
+        *grid_ctas = b->use_units ? b->band_grid : (b->prec == SCLBM_FP64 ? b->grid : b->grid_body[b->body]);
     return SCLBM_OK;
 }
 

@@ -18,7 +18,8 @@ struct TileRef {
 // block of the current tile's domain is copied into shared memory, so the tile
 // body reads its fields from there instead of holding the whole block in
 // registers.
-template <typename S, typename T, int FLAGS = KF_FORCE | KF_SOLID, bool AHEAD = false>
+template <typename S, typename T, int FLAGS = KF_FORCE | KF_SOLID, bool AHEAD = false,
+          bool COMPACT = false>
 __global__ void __launch_bounds__(BATCH_TX, (fused_min_ctas<T, AHEAD>()))
     k_batch2(const Fused2Args<S, T> *__restrict__ doms, const TileRef *__restrict__ tiles,
              int ntiles, int parity)
@@ -39,22 +40,29 @@ __global__ void __launch_bounds__(BATCH_TX, (fused_min_ctas<T, AHEAD>()))
             loaded = key;
         }
         // alternate march directions of a domain's row bands (see fused2_tile)
-        fused2_tile<S, T, BATCH_TX, false, FLAGS, false, AHEAD>(sa, tr.xb, tr.yb, s_rho, s_m,
-                                                                ((tr.yb / sa.tile_y) & 1) != 0);
+        const bool down = ((tr.yb / sa.tile_y) & 1) != 0;
+        if constexpr (COMPACT && (FLAGS & KF_SOLID) != 0) {
+            __shared__ CompactSmem<S, T, BATCH_TX> cs;
+            fused2_tile_compact<S, T, BATCH_TX, FLAGS>(sa, tr.xb, tr.yb, s_rho, s_m, cs, down);
+        } else {
+            fused2_tile<S, T, BATCH_TX, false, FLAGS, false, AHEAD>(sa, tr.xb, tr.yb, s_rho, s_m,
+                                                                    down);
+        }
         __syncthreads(); // the shared ring and block are reused by the next tile
     }
 }
 
 // flags: KF_FORCE / KF_SOLID when any domain of the batch has a volume force /
 // a solid node (the body drops what no domain needs)
-template <typename S, typename T, bool AHEAD = false>
+template <typename S, typename T, bool AHEAD = false, bool COMPACT = false>
 inline cudaError_t launch_batch_t(const Fused2Args<S, T> *doms, const TileRef *tiles, int ntiles,
                                   int parity, int grid, int flags, cudaStream_t s)
 {
     if (AHEAD || flags == (KF_FORCE | KF_SOLID))
-        k_batch2<S, T, KF_FORCE | KF_SOLID, AHEAD><<<grid, BATCH_TX, 0, s>>>(doms, tiles, ntiles, parity);
+        k_batch2<S, T, KF_FORCE | KF_SOLID, AHEAD, COMPACT><<<grid, BATCH_TX, 0, s>>>(doms, tiles,
+                                                                                  ntiles, parity);
     else if (flags == KF_SOLID)
-        k_batch2<S, T, KF_SOLID><<<grid, BATCH_TX, 0, s>>>(doms, tiles, ntiles, parity);
+        k_batch2<S, T, KF_SOLID, false, COMPACT><<<grid, BATCH_TX, 0, s>>>(doms, tiles, ntiles, parity);
     else if (flags == KF_FORCE)
         k_batch2<S, T, KF_FORCE><<<grid, BATCH_TX, 0, s>>>(doms, tiles, ntiles, parity);
     else
@@ -62,23 +70,24 @@ inline cudaError_t launch_batch_t(const Fused2Args<S, T> *doms, const TileRef *t
     return cudaGetLastError();
 }
 
-template <typename S, typename T, bool AHEAD = false> inline int batch_blocks_per_sm_t()
+template <typename S, typename T, bool AHEAD = false, bool COMPACT = false>
+inline int batch_blocks_per_sm_t()
 {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch2<S, T, KF_FORCE | KF_SOLID, AHEAD>,
-                                                      BATCH_TX, 0) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &n, k_batch2<S, T, KF_FORCE | KF_SOLID, AHEAD, COMPACT>, BATCH_TX, 0) != cudaSuccess)
         return 1;
     return n;
 }
 
-// `ahead` selects the load-ahead tile body (FP32 arithmetic only; ignored for FP64)
+// tile body of the FP32-arithmetic batches (ignored for FP64)
+enum BatchBody { BODY_TILE = 0, BODY_AHEAD = 1, BODY_COMPACT = 2 };
 cudaError_t launch_batch_fp64(const Fused2Args<double, double> *doms, const TileRef *tiles,
                               int ntiles, int parity, int grid, int flags, cudaStream_t s);
 cudaError_t launch_batch_f32(const Fused2Args<float, float> *doms, const TileRef *tiles,
-                             int ntiles, int parity, int grid, int flags, bool ahead, cudaStream_t s);
+                             int ntiles, int parity, int grid, int flags, int body, cudaStream_t s);
 cudaError_t launch_batch_f16(const Fused2Args<__half, float> *doms, const TileRef *tiles,
-                             int ntiles, int parity, int grid, int flags, bool ahead,
-                             cudaStream_t s);
-int batch_blocks_per_sm(sclbm_precision p, bool ahead = false);
+                             int ntiles, int parity, int grid, int flags, int body, cudaStream_t s);
+int batch_blocks_per_sm(sclbm_precision p, int body = BODY_TILE);
 
 } // namespace sclbm

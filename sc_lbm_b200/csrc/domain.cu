@@ -327,7 +327,7 @@ static cudaError_t step_one(const sclbm_domain *d, cudaStream_t s)
     }
     // variant 1: two pass; 4: register tile with L2 row prefetch; variant 2
     // (and the FP16 form): register-tile single pass
-    const int v = d->variant == 1 || d->variant == 4 || d->variant == 5 ? d->variant : 0;
+    const int v = d->variant == 1 || d->variant >= 4 ? d->variant : 0;
     if constexpr (sizeof(S) == 8) return launch_fused2_fp64(a, v, d->tx, s);
     else if constexpr (sizeof(S) == 4) return launch_fused2_f32(a, v, d->tx, s);
     else return launch_fused2_f16(a, v, d->tx, s);
@@ -437,7 +437,7 @@ fail:
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y)
 {
     if (!d) return set_error(SCLBM_E_INVALID_ARGUMENT, "null domain");
-    if (variant < 0 || variant > 5) return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0..5");
+    if (variant < 0 || variant > 6) return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0..6");
     if (tile_y < 0 || tile_y > 4096) return set_error(SCLBM_E_INVALID_ARGUMENT, "bad tile_y");
     if (variant == 1 && !d->rho_tmp[0] && d->ncomp == 2) {
         const size_t es = d->prec == SCLBM_FP64 ? 8 : 4;

@@ -423,6 +423,147 @@ __device__ __forceinline__ void fused2_tile_ahead(const Fused2Args<S, T> &a, con
     }
 }
 
+// Compacted fluid lanes (lattices with solid nodes).  Loading a row stays one
+// column per thread, but the row's populations are also published in shared
+// memory together with a per-warp ballot of its fluid interior columns; the
+// collision of that row (next iteration) is then done by threads 0..F-1 for
+// its F fluid nodes, thread j taking the j-th one.  Warps whose lanes would
+// all sit on solid nodes skip the collision and the remaining warps run full,
+// instead of every warp carrying its solid lanes idle through the collision.
+// Three population slots: iteration q publishes row q while row q-1 is being
+// collided, and row q+1 (written by a thread already in iteration q+1) never
+// lands on row q-1's slot.  Same arithmetic per node, same single writes.
+// bit index of the n-th (0-based) set bit of v; v has more than n bits set
+__device__ __forceinline__ int nth_set_bit(uint32_t v, int n)
+{
+    int pos = 0;
+#pragma unroll
+    for (int sh = 16; sh > 0; sh >>= 1) {
+        const uint32_t lo = v & ((1u << sh) - 1u);
+        const int c = __popc(lo);
+        if (n >= c) {
+            n -= c;
+            v >>= sh;
+            pos += sh;
+        } else {
+            v = lo;
+        }
+    }
+    return pos;
+}
+
+template <typename S, typename T, int TX> struct CompactSmem {
+    T pop[3][18][TX];          // populations of the last rows, [k*9 + i][column]
+    uint32_t ballot[3][TX / 32]; // fluid interior columns of those rows, per warp
+};
+
+template <typename S, typename T, int TX, int FLAGS>
+__device__ __forceinline__ void fused2_tile_compact(const Fused2Args<S, T> &a, const int xb,
+                                                    const int yb, T (&s_rho)[2][4][TX],
+                                                    uint8_t (&s_m)[4][TX],
+                                                    CompactSmem<S, T, TX> &cs, const bool down)
+{
+    static_assert((FLAGS & KF_SOLID) != 0, "compaction is for lattices with solid nodes");
+    constexpr int W = TX - 2, NW = TX / 32;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int nx = a.nx, ny = a.ny;
+    const int ncol = min(W, nx - xb);
+    const int nrow = min(a.tile_y, ny - yb);
+    const bool active = t <= ncol + 1;
+    const bool interior = t >= 1 && t <= ncol;
+    const int x = wrap1(xb - 1 + t, nx);
+    auto phys = [&](int q) { return down ? nrow - 1 - q : q; };
+
+    uint8_t m_ahead = 1;
+    if (active) m_ahead = a.mask[(uint32_t)wrap1(yb + phys(-1), ny) * (uint32_t)nx + (uint32_t)x];
+
+    T cur[2][9];
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+#pragma unroll
+        for (int i = 0; i < 9; ++i) cur[k][i] = T(0);
+
+    for (int q = -1; q <= nrow; ++q) {
+        const int r = phys(q);
+        const int y = wrap1(yb + r, ny);
+        const int slot = (q + 1) & 3, ps = (q + 1) % 3;
+        T rho[2] = {T(0), T(0)};
+        uint8_t m = 0;
+        if (active) {
+            const uint32_t node = (uint32_t)y * (uint32_t)nx + (uint32_t)x;
+            m = m_ahead;
+            if (q < nrow)
+                m_ahead = a.mask[(uint32_t)wrap1(yb + phys(q + 1), ny) * (uint32_t)nx + (uint32_t)x];
+            if (m || !a.solids_zero) {
+#pragma unroll
+                for (int k = 0; k < 2; ++k)
+#pragma unroll
+                    for (int i = 0; i < 9; ++i)
+                        cur[k][i] = T(Store<S>::ld(a.fin[k] + (size_t)i * a.N + node));
+            }
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                T sum = T(0); // 0.0 + f0 + ... + f8, src/fluid.cpp:177-181
+#pragma unroll
+                for (int i = 0; i < 9; ++i) sum += cur[k][i];
+                rho[k] = m ? sum : T(0);
+            }
+            if (!m && interior && !a.solids_zero && r >= 0 && r < nrow) {
+                // caller-owned arrays: the reference's stream leaves zeros at solids
+#pragma unroll
+                for (int k = 0; k < 2; ++k)
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) Store<S>::st(a.fout[k] + (size_t)i * a.N + node, T(0));
+            }
+        }
+        s_rho[0][slot][t] = rho[0];
+        s_rho[1][slot][t] = rho[1];
+        s_m[slot][t] = m;
+        const bool work = interior && m && r >= 0 && r < nrow;
+        if (work) {
+#pragma unroll
+            for (int k = 0; k < 2; ++k)
+#pragma unroll
+                for (int i = 0; i < 9; ++i) cs.pop[ps][k * 9 + i][t] = cur[k][i];
+        }
+        const uint32_t bal = __ballot_sync(0xffffffffu, work);
+        if (lane == 0) cs.ballot[ps][warp] = bal;
+        __syncthreads();
+
+        if (q >= 1) {
+            // the j-th fluid interior column of row phys(q-1), j = t
+            const int pp = q % 3;
+            int j = t, w = 0;
+            uint32_t b = 0;
+#pragma unroll
+            for (int v = 0; v < NW; ++v) {
+                const uint32_t bv = cs.ballot[pp][v];
+                const int c = __popc(bv);
+                if (w == v && j >= c) {
+                    j -= c;
+                    ++w;
+                } else if (w == v) {
+                    b = bv;
+                }
+            }
+            if (w < NW) {
+                const int col = w * 32 + nth_set_bit(b, j);
+                const int xc = wrap1(xb - 1 + col, nx);
+                const int s_old = (q - 1) & 3, sc = q & 3, s_new = (q + 1) & 3;
+                const int sb = down ? s_new : s_old, sa = down ? s_old : s_new;
+                const int yc = wrap1(yb + phys(q - 1), ny);
+                const Stencil<T> st{{s_rho[0][sb], s_rho[0][sc], s_rho[0][sa]},
+                                    {s_rho[1][sb], s_rho[1][sc], s_rho[1][sa]},
+                                    {s_m[sb], s_m[sc], s_m[sa]}, col};
+                const Nbr n = make_nbr(nx, xc, wrap1(xc - 1, nx), wrap1(xc + 1, nx), yc,
+                                       wrap1(yc - 1, ny), wrap1(yc + 1, ny));
+                const RingPops<T, T, TX> f{&cs.pop[pp][0][col]};
+                collide_push<S, T, FLAGS>(a, f, st, n);
+            }
+        }
+    }
+}
+
 // Tiles march up their rows (down = false) or down them (down = true).  The
 // launches give vertically neighbouring tiles opposite directions, so the two
 // rows a pair of tiles both read (each one's halo row is the other's edge row)
@@ -552,15 +693,21 @@ template <typename T, bool AHEAD> constexpr int fused_min_ctas()
 }
 
 template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS, bool PF = false,
-          bool AHEAD = false>
+          bool AHEAD = false, bool COMPACT = false>
 __global__ void __launch_bounds__(TX, (fused_min_ctas<T, AHEAD>()))
     k_fused2(const __grid_constant__ Fused2Args<S, T> a)
 {
     __shared__ T s_rho[2][4][TX];
     __shared__ uint8_t s_m[4][TX];
-    fused2_tile<S, T, TX, TWO_PASS, FLAGS, PF, AHEAD>(a, blockIdx.x * (TX - 2),
-                                                      blockIdx.y * a.tile_y, s_rho, s_m,
-                                                      (blockIdx.y & 1) != 0);
+    if constexpr (COMPACT && (FLAGS & KF_SOLID) != 0 && !TWO_PASS) {
+        __shared__ CompactSmem<S, T, TX> cs;
+        fused2_tile_compact<S, T, TX, FLAGS>(a, blockIdx.x * (TX - 2), blockIdx.y * a.tile_y, s_rho,
+                                             s_m, cs, (blockIdx.y & 1) != 0);
+    } else {
+        fused2_tile<S, T, TX, TWO_PASS, FLAGS, PF, AHEAD>(a, blockIdx.x * (TX - 2),
+                                                          blockIdx.y * a.tile_y, s_rho, s_m,
+                                                          (blockIdx.y & 1) != 0);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -668,30 +815,32 @@ template <typename S, typename T> inline int kernel_flags(const Fused2Args<S, T>
     return (a.c[0].force_on || a.c[1].force_on ? KF_FORCE : 0) | (a.has_solid ? KF_SOLID : 0);
 }
 
-template <typename S, typename T, int TX, bool TWO, int FLAGS, bool PF = false, bool AHEAD = false>
+template <typename S, typename T, int TX, bool TWO, int FLAGS, bool PF = false, bool AHEAD = false,
+          bool COMPACT = false>
 inline cudaError_t launch_fused2_f(const Fused2Args<S, T> &a, cudaStream_t s)
 {
     constexpr int W = TX - 2;
     const dim3 grid((a.nx + W - 1) / W, (a.ny + a.tile_y - 1) / a.tile_y);
-    k_fused2<S, T, TX, TWO, FLAGS, PF, AHEAD><<<grid, TX, 0, s>>>(a);
+    k_fused2<S, T, TX, TWO, FLAGS, PF, AHEAD, COMPACT><<<grid, TX, 0, s>>>(a);
     return cudaGetLastError();
 }
 
-template <typename S, typename T, int TX, bool PF = false, bool AHEAD = false>
+template <typename S, typename T, int TX, bool PF = false, bool AHEAD = false, bool COMPACT = false>
 inline cudaError_t launch_fused2_tx(const Fused2Args<S, T> &a, bool two_pass, cudaStream_t s)
 {
     if (two_pass) return launch_fused2_f<S, T, TX, true, KF_FORCE | KF_SOLID>(a, s);
     switch (kernel_flags(a)) {
     case 0: return launch_fused2_f<S, T, TX, false, 0, PF, AHEAD>(a, s);
     case KF_FORCE: return launch_fused2_f<S, T, TX, false, KF_FORCE, PF, AHEAD>(a, s);
-    case KF_SOLID: return launch_fused2_f<S, T, TX, false, KF_SOLID, PF, AHEAD>(a, s);
-    default: return launch_fused2_f<S, T, TX, false, KF_FORCE | KF_SOLID, PF, AHEAD>(a, s);
+    case KF_SOLID: return launch_fused2_f<S, T, TX, false, KF_SOLID, PF, AHEAD, COMPACT>(a, s);
+    default: return launch_fused2_f<S, T, TX, false, KF_FORCE | KF_SOLID, PF, AHEAD, COMPACT>(a, s);
     }
 }
 
 // variant 1: two pass; 4: single pass with L2 row prefetch (128 threads);
-// 5: single pass with loads one row ahead (128 threads); otherwise the
-// single-pass register tile
+// 5: single pass with loads one row ahead (128 threads); 6: single pass with
+// the collision on compacted fluid lanes (lattices with solid nodes; 128
+// threads); otherwise the single-pass register tile
 template <typename S, typename T>
 inline cudaError_t launch_fused2_any(const Fused2Args<S, T> &a, int variant, int tx,
                                      cudaStream_t s)
@@ -701,6 +850,11 @@ inline cudaError_t launch_fused2_any(const Fused2Args<S, T> &a, int variant, int
     if (tx == 64) return launch_fused2_tx<S, T, 64>(a, two, s);
     if (variant == 4) return launch_fused2_tx<S, T, 128, true>(a, false, s);
     if (variant == 5) return launch_fused2_tx<S, T, 128, false, true>(a, false, s);
+    if (variant == 6) {
+        // FP64's three population rows would exceed the static shared memory
+        if constexpr (sizeof(T) == 4) return launch_fused2_tx<S, T, 128, false, false, true>(a, false, s);
+        else return launch_fused2_tx<S, T, 128>(a, false, s);
+    }
     return launch_fused2_tx<S, T, 128>(a, two, s);
 }
 

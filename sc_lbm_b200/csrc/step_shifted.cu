@@ -44,28 +44,36 @@ cudaError_t launch_density_f16(const uint8_t *mask, const __half *f0, const __ha
 #include "batch_kernel.cuh"
 namespace sclbm {
 cudaError_t launch_batch_f32(const Fused2Args<float, float> *doms, const TileRef *tiles,
-                             int ntiles, int parity, int grid, int flags, bool ahead, cudaStream_t s)
+                             int ntiles, int parity, int grid, int flags, int body, cudaStream_t s)
 {
-    if (ahead) return launch_batch_t<float, float, true>(doms, tiles, ntiles, parity, grid, flags, s);
+    if (body == BODY_AHEAD)
+        return launch_batch_t<float, float, true>(doms, tiles, ntiles, parity, grid, flags, s);
+    if (body == BODY_COMPACT)
+        return launch_batch_t<float, float, false, true>(doms, tiles, ntiles, parity, grid, flags, s);
     return launch_batch_t<float, float>(doms, tiles, ntiles, parity, grid, flags, s);
 }
 cudaError_t launch_batch_f16(const Fused2Args<__half, float> *doms, const TileRef *tiles,
-                             int ntiles, int parity, int grid, int flags, bool ahead,
-                             cudaStream_t s)
+                             int ntiles, int parity, int grid, int flags, int body, cudaStream_t s)
 {
-    if (ahead) return launch_batch_t<__half, float, true>(doms, tiles, ntiles, parity, grid, flags, s);
+    if (body == BODY_AHEAD)
+        return launch_batch_t<__half, float, true>(doms, tiles, ntiles, parity, grid, flags, s);
+    if (body == BODY_COMPACT)
+        return launch_batch_t<__half, float, false, true>(doms, tiles, ntiles, parity, grid, flags, s);
     return launch_batch_t<__half, float>(doms, tiles, ntiles, parity, grid, flags, s);
 }
 int batch_blocks_per_sm_fp64();
-int batch_blocks_per_sm(sclbm_precision p, bool ahead)
+int batch_blocks_per_sm(sclbm_precision p, int body)
 {
     switch (p) {
     case SCLBM_FP64: return batch_blocks_per_sm_fp64();
     case SCLBM_FP32_SHIFTED:
-        return ahead ? batch_blocks_per_sm_t<float, float, true>() : batch_blocks_per_sm_t<float, float>();
+        return body == BODY_AHEAD     ? batch_blocks_per_sm_t<float, float, true>()
+               : body == BODY_COMPACT ? batch_blocks_per_sm_t<float, float, false, true>()
+                                      : batch_blocks_per_sm_t<float, float>();
     default:
-        return ahead ? batch_blocks_per_sm_t<__half, float, true>()
-                     : batch_blocks_per_sm_t<__half, float>();
+        return body == BODY_AHEAD     ? batch_blocks_per_sm_t<__half, float, true>()
+               : body == BODY_COMPACT ? batch_blocks_per_sm_t<__half, float, false, true>()
+                                      : batch_blocks_per_sm_t<__half, float>();
     }
 }
 } // namespace sclbm

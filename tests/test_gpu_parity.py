@@ -145,7 +145,7 @@ def test_shifted_forms_density_error(sclbm, oracle, name, steps, prec, tol_max, 
 
 
 @pytest.mark.parametrize("variant,tile_y", [(1, 4), (4, 0), (4, 7), (3, 0), (5, 0), (5, 7),
-                                            (5, 1), (5, 2)])
+                                            (5, 1), (5, 2), (6, 0), (6, 1), (6, 5), (6, 64)])
 def test_shifted_variants_match_register_tile(sclbm, variant, tile_y):
     """The shifted forms give the same bytes with every kernel variant."""
     for prec in (sclbm.FP32_SHIFTED, sclbm.FP16_SHIFTED):
@@ -203,7 +203,8 @@ def test_batch_matches_individual_domains(sclbm):
     for prec, graph, kernel in ((sclbm.FP64, True, 0), (sclbm.FP32_SHIFTED, True, 0),
                                 (sclbm.FP32_SHIFTED, False, 3), (sclbm.FP64, False, 2),
                                 (sclbm.FP16_SHIFTED, False, 0), (sclbm.FP32_SHIFTED, True, 5),
-                                (sclbm.FP16_SHIFTED, False, 5)):
+                                (sclbm.FP16_SHIFTED, False, 5), (sclbm.FP32_SHIFTED, True, 6),
+                                (sclbm.FP16_SHIFTED, False, 6)):
         rr = (0.8, 1.2)
         solo = [gpu_runner.run_domain(sclbm, dict(RUNS[n], steps=45), prec, rho_ref=rr) for n in names]
         doms = [gpu_runner.make_domain(sclbm, RUNS[n], prec, rho_ref=rr) for n in names]

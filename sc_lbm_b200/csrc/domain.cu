@@ -81,26 +81,6 @@ __global__ void k_init_noise(size_t N, const uint8_t *__restrict__ mask, S *__re
     }
 }
 
-// Neighbour links of every node: bit i-1 set when the node along c_i
-// (periodic) is fluid.  Computed once per lattice; lets a fluid node whose
-// eight neighbours are all fluid take the all-fluid body of collide_push.
-__global__ void __launch_bounds__(256) k_links(int nx, int ny, const uint8_t *__restrict__ mask,
-                                               uint8_t *__restrict__ links)
-{
-    const size_t N = (size_t)nx * ny;
-    for (size_t n = blockIdx.x * (size_t)blockDim.x + threadIdx.x; n < N;
-         n += (size_t)gridDim.x * blockDim.x) {
-        const int x = int(n % nx), y = int(n / nx);
-        uint8_t b = 0;
-#pragma unroll
-        for (int i = 1; i < 9; ++i) {
-            const int xn = wrap1(x + cx(i), nx), yn = wrap1(y + cy(i), ny);
-            if (mask[(size_t)yn * nx + xn]) b |= uint8_t(1u << (i - 1));
-        }
-        links[n] = b;
-    }
-}
-
 // all nine populations of the solid nodes set to 0 (FP64 uploads)
 __global__ void k_zero_solids(size_t N, const uint8_t *__restrict__ mask, double *__restrict__ f)
 {
@@ -297,7 +277,6 @@ static void fill2(const sclbm_domain *d, Fused2Args<S, T> &a)
     a.solid_from_mask = 1;
     a.has_solid = d->has_solid ? 1 : 0;
     a.solids_zero = 1; // creation, uploads and initialisers write 0 at solid nodes
-    a.links = d->d_links;
 }
 
 void domain_fused2_args(const sclbm_domain *d, Fused2Args<double, double> *a64,
@@ -391,7 +370,6 @@ void sclbm_domain_destroy(sclbm_domain *d)
     for (auto *p : d->rho_tmp)
         if (p) cudaFree(p);
     if (d->d_mask) cudaFree(d->d_mask);
-    if (d->d_links) cudaFree(d->d_links);
     if (d->staging) cudaFree(d->staging);
     if (d->partials) cudaFree(d->partials);
     delete d;
@@ -444,20 +422,8 @@ int sclbm_domain_create(size_t nx, size_t ny, const int32_t *mask, const sclbm_p
     d->partial_blocks = sm_count() * 4;
     if ((rc = dom_alloc(d, (void **)&d->partials, (size_t)(d->partial_blocks + 1) * 8 * sizeof(double))))
         goto fail;
-    if (cudaMemcpyAsync(d->d_mask, hm.data(), N, cudaMemcpyHostToDevice, s) != cudaSuccess) {
-        rc = set_error(SCLBM_E_CUDA, "mask upload");
-        goto fail;
-    }
-    if (d->has_solid) {
-        // neighbour links for the interior-fluid fast path of the fused kernels
-        if ((rc = dom_alloc(d, (void **)&d->d_links, N))) goto fail;
-        k_links<<<grid_for(N, 256), 256, 0, s>>>((int)nx, (int)ny, d->d_mask, d->d_links);
-        if (cudaGetLastError() != cudaSuccess) {
-            rc = set_error(SCLBM_E_CUDA, "neighbour links");
-            goto fail;
-        }
-    }
-    if (cudaStreamSynchronize(s) != cudaSuccess) {
+    if (cudaMemcpyAsync(d->d_mask, hm.data(), N, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
         rc = set_error(SCLBM_E_CUDA, "mask upload");
         goto fail;
     }

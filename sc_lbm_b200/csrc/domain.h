@@ -8,7 +8,6 @@ struct sclbm_domain {
     sclbm_precision prec = SCLBM_FP64;
     sclbm_params p{};
     uint8_t *d_mask = nullptr;
-    uint8_t *d_links = nullptr; // neighbour-fluid bits per node (lattices with solids)
     void *buf[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}}; // [parity][comp], 9N each
     int parity = 0;                                             // buf[parity] holds the state
     void *rho_tmp[2] = {nullptr, nullptr}; // density arrays of the two-pass variant

@@ -148,13 +148,9 @@ __device__ __forceinline__ void push_one(const Fused2Args<S, T> &a, const int k,
 // sequence of src/lbm.cpp:177-204 (repulsive force), :250-269 (equilibrium
 // velocity), src/fluid.cpp:254-276 + src/lbm.cpp:305-311 (equilibrium, BGK),
 // :333-337 (volume force), :404-427 (stream with half-way bounce-back).
-// links: the node's neighbour-link byte (k_links), or -1 to read the mask
-// stencil.  A fluid node with all eight links runs the all-fluid body (the
-// same arithmetic: the solid sums are zero and nothing bounces back).
 template <typename S, typename T, int FLAGS, typename Pops>
 __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Pops &f,
-                                             const Stencil<T> &st, const Nbr &n,
-                                             const int links = -1)
+                                             const Stencil<T> &st, const Nbr &n)
 {
     constexpr bool EXACT = sizeof(T) == 8;
     constexpr bool FORCE = (FLAGS & KF_FORCE) != 0, SOLID = (FLAGS & KF_SOLID) != 0;
@@ -170,19 +166,13 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
         }
         return;
     }
-    if constexpr (SOLID) {
-        if (links == 0xFF) {
-            collide_push<S, T, FLAGS & ~KF_SOLID>(a, f, st, n);
-            return;
-        }
-    }
     bool nf[9];
     T p0[9], p1[9];
 #pragma unroll
     for (int i = 1; i < 9; ++i) {
         const int sl = cy(i) + 1;
         const int col = st.c + cx(i);
-        nf[i] = SOLID ? (links >= 0 ? ((links >> (i - 1)) & 1) != 0 : st.m[sl][col] != 0) : true;
+        nf[i] = SOLID ? st.m[sl][col] != 0 : true;
         p0[i] = st.r0[sl][col];
         p1[i] = st.r1[sl][col];
     }
@@ -607,12 +597,8 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
     // the mask of the next row is loaded one iteration ahead, so the population
     // loads of a row never wait on its mask load
     uint8_t m_ahead = 1;
-    int lk_ahead = -1, lk_cur = -1, lk_prev = -1; // links of rows q+1, q, q-1
-    if (SOLID && active) {
-        const uint32_t nd = (uint32_t)wrap1(yb + phys(-1), ny) * (uint32_t)nx + (uint32_t)x;
-        m_ahead = a.mask[nd];
-        if (a.links) lk_ahead = a.links[nd];
-    }
+    if (SOLID && active)
+        m_ahead = a.mask[(uint32_t)wrap1(yb + phys(-1), ny) * (uint32_t)nx + (uint32_t)x];
 
     // iteration q: load row phys(q) into cur, publish its density, collide row
     // phys(q-1) (prev) from the densities of rows phys(q-2), phys(q-1), phys(q)
@@ -639,12 +625,8 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
             const uint32_t node = (uint32_t)y * (uint32_t)nx + (uint32_t)x;
             if (SOLID) {
                 m = m_ahead;
-                lk_cur = lk_ahead;
-                if (q < nrow) {
-                    const uint32_t nd = (uint32_t)wrap1(yb + phys(q + 1), ny) * (uint32_t)nx + (uint32_t)x;
-                    m_ahead = a.mask[nd];
-                    if (a.links) lk_ahead = a.links[nd];
-                }
+                if (q < nrow)
+                    m_ahead = a.mask[(uint32_t)wrap1(yb + phys(q + 1), ny) * (uint32_t)nx + (uint32_t)x];
             }
             // solid nodes hold zeros on the domain path: nothing to read there
             const bool need_pops = (!TWO_PASS || (interior && r >= 0 && r < nrow)) &&
@@ -686,9 +668,8 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
                                 {s_rho[1][sb], s_rho[1][sc], s_rho[1][sa]},
                                 {s_m[sb], s_m[sc], s_m[sa]}, t};
             const Nbr n = make_nbr(nx, x, xl, xr, yc, wrap1(yc - 1, ny), wrap1(yc + 1, ny));
-            collide_push<S, T, FLAGS>(a, prev, st, n, lk_prev);
+            collide_push<S, T, FLAGS>(a, prev, st, n);
         }
-        lk_prev = lk_cur;
     };
 
     T A[2][9], B[2][9];

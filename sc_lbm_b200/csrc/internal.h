@@ -94,8 +94,6 @@ template <typename S, typename T> struct Fused2Args {
     int has_solid;                       // the mask has solid nodes (else all fluid)
     int solids_zero;                     // both buffers hold 0 at solid nodes: the kernels
                                          // neither read nor write them (domain path)
-    const uint8_t *__restrict__ links;   // per node, bit i-1: the neighbour along c_i is fluid
-                                         // (domain path; null: read the mask stencil)
 };
 
 // arguments of the single-component fused kernel

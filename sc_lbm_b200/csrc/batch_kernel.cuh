@@ -18,9 +18,12 @@ struct TileRef {
 // block of the current tile's domain is copied into shared memory, so the tile
 // body reads its fields from there instead of holding the whole block in
 // registers.
+// Five resident CTAs per SM (102 registers): the tile loop and the shared
+// argument block leave the six-CTA cap of the single-domain kernel spilling,
+// and on the 512-domain ensemble the five-CTA form ran 13 % faster.
 template <typename S, typename T, int FLAGS = KF_FORCE | KF_SOLID, bool AHEAD = false,
           bool COMPACT = false>
-__global__ void __launch_bounds__(BATCH_TX, (fused_min_ctas<T, AHEAD>()))
+__global__ void __launch_bounds__(BATCH_TX, (sizeof(T) == 8 ? 1 : 5))
     k_batch2(const Fused2Args<S, T> *__restrict__ doms, const TileRef *__restrict__ tiles,
              int ntiles, int parity)
 {
@@ -58,11 +61,11 @@ template <typename S, typename T, bool AHEAD = false, bool COMPACT = false>
 inline cudaError_t launch_batch_t(const Fused2Args<S, T> *doms, const TileRef *tiles, int ntiles,
                                   int parity, int grid, int flags, cudaStream_t s)
 {
-    if (AHEAD || flags == (KF_FORCE | KF_SOLID))
+    // batches with solid nodes run the force + solid body (the force vector is
+    // zero where no force is set); it compiled leaner than the solid-only one
+    if (AHEAD || (flags & KF_SOLID))
         k_batch2<S, T, KF_FORCE | KF_SOLID, AHEAD, COMPACT><<<grid, BATCH_TX, 0, s>>>(doms, tiles,
                                                                                   ntiles, parity);
-    else if (flags == KF_SOLID)
-        k_batch2<S, T, KF_SOLID, false, COMPACT><<<grid, BATCH_TX, 0, s>>>(doms, tiles, ntiles, parity);
     else if (flags == KF_FORCE)
         k_batch2<S, T, KF_FORCE><<<grid, BATCH_TX, 0, s>>>(doms, tiles, ntiles, parity);
     else

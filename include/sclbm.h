@@ -243,8 +243,8 @@ int sclbm_domain_step(sclbm_domain *d, int nsteps);
  * FP64 (out[3*comp + 0..2]); out[6] = number of non-finite populations. */
 int sclbm_domain_mass_momentum(sclbm_domain *d, double out[7]);
 /* Kernel selection (all variants give identical results):
- *   0 = automatic (default): the fastest measured form for the storage
- *       precision -- 3 for FP64, 2 for FP32 and FP16;
+ *   0 = automatic (default): the fastest measured form -- 3 for FP64
+ *       storage on lattices with solid nodes, 2 otherwise;
  *   1 = two pass (density kernel, then the fused kernel reading it);
  *   2 = single pass, one tile per CTA, population rows held in registers;
  *   3 = single pass, population rows staged through a shared-memory ring by

@@ -318,9 +318,11 @@ static cudaError_t step_one(const sclbm_domain *d, cudaStream_t s)
                                    (float *)d->rho_tmp[1], d->N, s);
         if (e != cudaSuccess) return e;
     }
-    // variant 0 picks the fastest measured form: pipelined for FP64 storage,
-    // register tile for FP32/FP16; 3 forces the pipelined kernel
-    const bool pipelined = d->variant == 3 || (d->variant == 0 && sizeof(S) == 8);
+    // variant 0 picks the fastest measured form on B200: the register tile,
+    // except for FP64 storage on a lattice with solid nodes, where the pipelined
+    // kernel is faster (4096^2: 16.98 vs 16.55 GLUPS all-fluid; 13.6 vs 11.4 at
+    // 60 % fluid); 3 forces the pipelined kernel
+    const bool pipelined = d->variant == 3 || (d->variant == 0 && sizeof(S) == 8 && d->has_solid);
     if (pipelined) {
         if constexpr (sizeof(S) == 8) return launch_fused2_async_fp64(a, s);
         else if constexpr (sizeof(S) == 4) return launch_fused2_async_f32(a, s);

@@ -208,5 +208,19 @@ def all_cases() -> dict:
     return c
 
 
+def long_cases() -> dict:
+    """Full-size runs whose reference results take minutes on the CPU: pinned
+    by digests of the compiled reference only (no oracle re-run in the CPU
+    suite); the GPU suite compares its FP64 results with them bit for bit."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
+    from sc_lbm_b200 import workloads as W
+    w = W.laplace(40.0)   # configuration 2: 256 x 256, disk of radius 40, G = 0.9, +-1e-3 noise
+    return {"laplace_256x256_r40_20k": dict(
+        nx=256, ny=256, geom=[], mode="two", fluid1=(1.0, 0.9, 0.0), fluid2=(1.0, 0.9, 0.0),
+        init=("file", np.concatenate([w["f1"], w["f2"]])), force=(0, [0.0] * 9), steps=20000)}
+
+
 # cases whose full arrays are committed (small enough to diagnose a mismatch)
 FULL_ARRAY_CASES = ("x_walls_20x10_uni", "ops1_y_walls_20x10", "absent_24x16", "empty_5x10_multi")

@@ -37,7 +37,7 @@ def main() -> None:
     if not pyoracle.have_ref():
         pyoracle.build(ref=True)
     out, arrays = {}, {}
-    for name, case in cases.all_cases().items():
+    for name, case in list(cases.all_cases().items()) + list(cases.long_cases().items()):
         res = pyoracle.run_ref(case)
         out[name] = {k: [digest(v), int(v.size)] for k, v in sorted(res.items())}
         if name in cases.FULL_ARRAY_CASES:

@@ -102,3 +102,16 @@ def test_poiseuille_10k_reference_and_analytic(sclbm):
     # 10,000 steps are 0.72 viscous times (H^2/nu): the slowest mode has decayed
     # to ~1e-3, and the reference's u = j/rho omits the half-force shift
     assert np.linalg.norm(u[1:-1] - ua) / np.linalg.norm(ua) < 5e-3
+
+
+def test_laplace_full_size_fp64_matches_reference(sclbm):
+    """Configuration 2 at full size (256 x 256, radius 40, 20,000 steps): the
+    fused FP64 step on fluid objects and the FP64 domain reproduce the
+    compiled reference's populations and final fields bit for bit."""
+    import gpu_runner
+    name = "laplace_256x256_r40_20k"
+    case = cases.long_cases()[name]
+    want = DIGESTS[name]
+    for res in (gpu_runner.run_fused(sclbm, case), gpu_runner.run_domain(sclbm, case, sclbm.FP64)):
+        for k in ("c1_f", "c2_f", "c1_rho_final", "c2_rho_final", "c1_ux_final", "c2_uy_final"):
+            assert _digest(res[k]) == want[k][0], k

@@ -256,8 +256,10 @@ int sclbm_domain_mass_momentum(sclbm_domain *d, double out[7]);
  *       (a third row buffer in registers), 128 threads per tile;
  *   6 = variant 2 with each row's collision done by consecutive threads on
  *       its fluid nodes only (populations staged in shared memory), for
- *       lattices with solid nodes (all-fluid lattices run variant 2).
- * tile_y = rows per tile of variants 1, 2, 4, 5 and 6 (0 keeps the default). */
+ *       lattices with solid nodes (all-fluid lattices run variant 2);
+ *   7 = variant 2 with 64-bit element offsets (what lattices of 2^32/9 nodes
+ *       and more always run; the other variants use 32-bit offsets).
+ * tile_y = rows per tile of variants 1, 2 and 4-7 (0 keeps the default). */
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y);
 /* Threads per tile of the register-tile kernel (variants 1, 2): 64 or 128. */
 int sclbm_domain_set_threads(sclbm_domain *d, int tx);

@@ -131,6 +131,11 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
             return set_error(SCLBM_E_INVALID_ARGUMENT,
                              "batch domains must be two-component, of one precision and in step");
         }
+        if (needs_wide_offsets(d->N)) {
+            sclbm_batch_destroy(b);
+            return set_error(SCLBM_E_INVALID_ARGUMENT,
+                             "batch domains must have fewer than 2^32/9 nodes (step larger ones alone)");
+        }
         if (d->has_solid) b->flags |= KF_SOLID;
         if (d->p.force_on[0] || d->p.force_on[1]) b->flags |= KF_FORCE;
         const SclbmTunedShape ts = tuned_shape(d->nx, d->ny, b->prec);

@@ -439,7 +439,7 @@ fail:
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y)
 {
     if (!d) return set_error(SCLBM_E_INVALID_ARGUMENT, "null domain");
-    if (variant < 0 || variant > 6) return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0..6");
+    if (variant < 0 || variant > 7) return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0..7");
     if (tile_y < 0 || tile_y > 4096) return set_error(SCLBM_E_INVALID_ARGUMENT, "bad tile_y");
     if (variant == 1 && !d->rho_tmp[0] && d->ncomp == 2) {
         const size_t es = d->prec == SCLBM_FP64 ? 8 : 4;

@@ -135,7 +135,7 @@ __device__ __forceinline__ void async_segment(const Fused2Args<S, T> &a, const i
                                 {rho + (1 * 4 + sm) * P, rho + (1 * 4 + sc) * P, rho + (1 * 4 + sp) * P},
                                 {msk + sm * P, msk + sc * P, msk + sp * P}, t + 1};
             const Nbr n = make_nbr(nx, x, xl, xr, yc, wrap1(yc - 1, ny), wrap1(yc + 1, ny));
-            collide_push<S, T, FLAGS>(a, f, st, n);
+            collide_push<S, T, FLAGS, true>(a, f, st, n); // 64-bit offsets: any lattice size
         }
         // row lr-1's stage is free again: request row lr+R-1 into it
         issue(lr + R - 1);

@@ -34,6 +34,7 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "internal.h"
 #include "lattice.cuh"
@@ -131,14 +132,24 @@ __device__ __forceinline__ Nbr make_nbr(const int nx, const int x, const int xl,
 // fluid node, else back into the opposite direction at the node itself.  The
 // destination is selected, not branched on, so warps with both kinds of
 // nodes issue one store per population.
-template <typename S, typename T, bool SOLID>
+// Element offsets i*N + node in 32 bits (one integer multiply-add per access)
+// when the nine arrays of a component hold fewer than 2^32 elements; WIDE
+// kernels, launched for larger lattices, compute them in 64 bits.
+template <bool WIDE> using Off = std::conditional_t<WIDE, size_t, uint32_t>;
+template <bool WIDE> __device__ __forceinline__ Off<WIDE> elem(int i, size_t N, uint32_t node)
+{
+    return (Off<WIDE>)i * (Off<WIDE>)N + (Off<WIDE>)node;
+}
+inline bool needs_wide_offsets(size_t N) { return 9 * (unsigned long long)N >= (1ull << 32); }
+
+template <typename S, typename T, bool SOLID, bool WIDE = false>
 __device__ __forceinline__ void push_one(const Fused2Args<S, T> &a, const int k, const int i,
                                          const T v, const bool nf, const Nbr &n)
 {
     if (i == 0 || !SOLID) {
-        Store<S>::st(a.fout[k] + (size_t)i * a.N + n.nb[i], v);
+        Store<S>::st(a.fout[k] + elem<WIDE>(i, a.N, n.nb[i]), v);
     } else {
-        const size_t off = nf ? (size_t)i * a.N + n.nb[i] : (size_t)opp(i) * a.N + n.nb[0];
+        const Off<WIDE> off = nf ? elem<WIDE>(i, a.N, n.nb[i]) : elem<WIDE>(opp(i), a.N, n.nb[0]);
         Store<S>::st(a.fout[k] + off, v);
     }
 }
@@ -148,7 +159,7 @@ __device__ __forceinline__ void push_one(const Fused2Args<S, T> &a, const int k,
 // sequence of src/lbm.cpp:177-204 (repulsive force), :250-269 (equilibrium
 // velocity), src/fluid.cpp:254-276 + src/lbm.cpp:305-311 (equilibrium, BGK),
 // :333-337 (volume force), :404-427 (stream with half-way bounce-back).
-template <typename S, typename T, int FLAGS, typename Pops>
+template <typename S, typename T, int FLAGS, bool WIDE = false, typename Pops>
 __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Pops &f,
                                              const Stencil<T> &st, const Nbr &n)
 {
@@ -162,7 +173,7 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
 #pragma unroll
             for (int k = 0; k < 2; ++k)
 #pragma unroll
-                for (int i = 0; i < 9; ++i) Store<S>::st(a.fout[k] + (size_t)i * a.N + node, T(0));
+                for (int i = 0; i < 9; ++i) Store<S>::st(a.fout[k] + elem<WIDE>(i, a.N, node), T(0));
         }
         return;
     }
@@ -239,7 +250,7 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
                 if constexpr (FORCE) {
                     if (a.c[k].force_on) v += a.c[k].force[i];
                 }
-                push_one<S, T, SOLID>(a, k, i, v, nf[i], n);
+                push_one<S, T, SOLID, WIDE>(a, k, i, v, nf[i], n);
             }
         }
     } else {
@@ -306,7 +317,7 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
                 float v = fmaf(om, fe - fi, fi);
                 // the force vector is zero for a component without a volume force
                 if constexpr (FORCE) v += a.c[k].force[i];
-                push_one<S, T, SOLID>(a, k, i, v, nf[i], n);
+                push_one<S, T, SOLID, WIDE>(a, k, i, v, nf[i], n);
             }
         }
     }
@@ -362,7 +373,7 @@ __device__ __forceinline__ void fused2_tile_ahead(const Fused2Args<S, T> &a, con
             for (int k = 0; k < 2; ++k)
 #pragma unroll
                 for (int i = 0; i < 9; ++i)
-                    buf[k][i] = T(Store<S>::ld(a.fin[k] + (size_t)i * a.N + node));
+                    buf[k][i] = T(Store<S>::ld(a.fin[k] + elem<false>(i, a.N, node)));
         }
     };
 
@@ -499,7 +510,7 @@ __device__ __forceinline__ void fused2_tile_compact(const Fused2Args<S, T> &a, c
                 for (int k = 0; k < 2; ++k)
 #pragma unroll
                     for (int i = 0; i < 9; ++i)
-                        cur[k][i] = T(Store<S>::ld(a.fin[k] + (size_t)i * a.N + node));
+                        cur[k][i] = T(Store<S>::ld(a.fin[k] + elem<false>(i, a.N, node)));
             }
 #pragma unroll
             for (int k = 0; k < 2; ++k) {
@@ -513,7 +524,7 @@ __device__ __forceinline__ void fused2_tile_compact(const Fused2Args<S, T> &a, c
 #pragma unroll
                 for (int k = 0; k < 2; ++k)
 #pragma unroll
-                    for (int i = 0; i < 9; ++i) Store<S>::st(a.fout[k] + (size_t)i * a.N + node, T(0));
+                    for (int i = 0; i < 9; ++i) Store<S>::st(a.fout[k] + elem<false>(i, a.N, node), T(0));
             }
         }
         s_rho[0][slot][t] = rho[0];
@@ -572,7 +583,7 @@ __device__ __forceinline__ void fused2_tile_compact(const Fused2Args<S, T> &a, c
 // Direction changes only the order of the rows; every node gets the same
 // arithmetic and every destination slot the same single write.
 template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS, bool PF = false,
-          bool AHEAD = false>
+          bool AHEAD = false, bool WIDE = false>
 __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int xb, const int yb,
                                             T (&s_rho)[2][4][TX], uint8_t (&s_m)[4][TX],
                                             const bool down = false)
@@ -636,7 +647,7 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
                 for (int k = 0; k < 2; ++k)
 #pragma unroll
                     for (int i = 0; i < 9; ++i)
-                        cur[k][i] = T(Store<S>::ld(a.fin[k] + (size_t)i * a.N + node));
+                        cur[k][i] = T(Store<S>::ld(a.fin[k] + elem<WIDE>(i, a.N, node)));
             }
             if (TWO_PASS) {
                 rho[0] = a.rho_in[0][node];
@@ -668,7 +679,7 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
                                 {s_rho[1][sb], s_rho[1][sc], s_rho[1][sa]},
                                 {s_m[sb], s_m[sc], s_m[sa]}, t};
             const Nbr n = make_nbr(nx, x, xl, xr, yc, wrap1(yc - 1, ny), wrap1(yc + 1, ny));
-            collide_push<S, T, FLAGS>(a, prev, st, n);
+            collide_push<S, T, FLAGS, WIDE>(a, prev, st, n);
         }
     };
 
@@ -693,7 +704,7 @@ template <typename T, bool AHEAD> constexpr int fused_min_ctas()
 }
 
 template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS, bool PF = false,
-          bool AHEAD = false, bool COMPACT = false>
+          bool AHEAD = false, bool COMPACT = false, bool WIDE = false>
 __global__ void __launch_bounds__(TX, (fused_min_ctas<T, AHEAD>()))
     k_fused2(const __grid_constant__ Fused2Args<S, T> a)
 {
@@ -704,9 +715,9 @@ __global__ void __launch_bounds__(TX, (fused_min_ctas<T, AHEAD>()))
         fused2_tile_compact<S, T, TX, FLAGS>(a, blockIdx.x * (TX - 2), blockIdx.y * a.tile_y, s_rho,
                                              s_m, cs, (blockIdx.y & 1) != 0);
     } else {
-        fused2_tile<S, T, TX, TWO_PASS, FLAGS, PF, AHEAD>(a, blockIdx.x * (TX - 2),
-                                                          blockIdx.y * a.tile_y, s_rho, s_m,
-                                                          (blockIdx.y & 1) != 0);
+        fused2_tile<S, T, TX, TWO_PASS, FLAGS, PF, AHEAD, WIDE>(a, blockIdx.x * (TX - 2),
+                                                                blockIdx.y * a.tile_y, s_rho, s_m,
+                                                                (blockIdx.y & 1) != 0);
     }
 }
 
@@ -816,12 +827,12 @@ template <typename S, typename T> inline int kernel_flags(const Fused2Args<S, T>
 }
 
 template <typename S, typename T, int TX, bool TWO, int FLAGS, bool PF = false, bool AHEAD = false,
-          bool COMPACT = false>
+          bool COMPACT = false, bool WIDE = false>
 inline cudaError_t launch_fused2_f(const Fused2Args<S, T> &a, cudaStream_t s)
 {
     constexpr int W = TX - 2;
     const dim3 grid((a.nx + W - 1) / W, (a.ny + a.tile_y - 1) / a.tile_y);
-    k_fused2<S, T, TX, TWO, FLAGS, PF, AHEAD, COMPACT><<<grid, TX, 0, s>>>(a);
+    k_fused2<S, T, TX, TWO, FLAGS, PF, AHEAD, COMPACT, WIDE><<<grid, TX, 0, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -846,6 +857,10 @@ inline cudaError_t launch_fused2_any(const Fused2Args<S, T> &a, int variant, int
                                      cudaStream_t s)
 {
     if (a.tile_y < 1 || a.nx < 1 || a.ny < 1) return cudaErrorInvalidValue;
+    // 64-bit offsets (lattices of 2^32/9 nodes and more; variant 7 asks for
+    // them on any lattice): the general single-pass kernel
+    if (needs_wide_offsets(a.N) || variant == 7)
+        return launch_fused2_f<S, T, 128, false, KF_FORCE | KF_SOLID, false, false, false, true>(a, s);
     const bool two = variant == 1;
     if (tx == 64) return launch_fused2_tx<S, T, 64>(a, two, s);
     if (variant == 4) return launch_fused2_tx<S, T, 128, true>(a, false, s);

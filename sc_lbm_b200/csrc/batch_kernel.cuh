@@ -27,7 +27,7 @@ __global__ void __launch_bounds__(BATCH_TX, (sizeof(T) == 8 ? 1 : 5))
     k_batch2(const Fused2Args<S, T> *__restrict__ doms, const TileRef *__restrict__ tiles,
              int ntiles, int parity)
 {
-    __shared__ T s_rho[2][4][BATCH_TX];
+    __shared__ V2<T> s_rho[4][BATCH_TX];
     __shared__ uint8_t s_m[4][BATCH_TX];
     __shared__ __align__(16) Fused2Args<S, T> sa;
     static_assert(sizeof(Fused2Args<S, T>) % 4 == 0, "argument block copied as words");

@@ -49,7 +49,7 @@ __device__ __forceinline__ void async_copy_node(S *pops, int stage, int col,
 
 template <typename S, typename T, int TX, int R>
 __device__ __forceinline__ void async_density(const S *pops, int stage, int col, uint8_t m,
-                                              T *rho, uint8_t *msk, int slot)
+                                              V2<T> *rho, uint8_t *msk, int slot)
 {
     constexpr int P = TX + 2;
     T r[2];
@@ -60,8 +60,7 @@ __device__ __forceinline__ void async_density(const S *pops, int stage, int col,
         for (int i = 0; i < 9; ++i) s += T(pops[((stage * 2 + k) * 9 + i) * P + col]);
         r[k] = m ? s : T(0);
     }
-    rho[(0 * 4 + slot) * P + col] = r[0];
-    rho[(1 * 4 + slot) * P + col] = r[1];
+    rho[slot * P + col] = Vec2<T>::make(r[0], r[1]);
     msk[slot * P + col] = m;
 }
 
@@ -74,7 +73,8 @@ __device__ __forceinline__ void async_segment(const Fused2Args<S, T> &a, const i
     constexpr int P = L::P;
     constexpr bool SOLID = (FLAGS & KF_SOLID) != 0;
     S *pops = reinterpret_cast<S *>(smem);
-    T *rho = reinterpret_cast<T *>(smem + L::pops);
+    V2<T> *rho = reinterpret_cast<V2<T> *>(smem + L::pops);
+    static_assert(L::pops % sizeof(V2<T>) == 0, "density ring alignment");
     uint8_t *msk = smem + L::pops + L::rho;
 
     const int t = threadIdx.x;
@@ -131,8 +131,7 @@ __device__ __forceinline__ void async_segment(const Fused2Args<S, T> &a, const i
             const int yc = wrap1(y0 + lr - 2, ny);
             const int sm = (lr - 2) & 3, sc = (lr - 1) & 3, sp = slot;
             const RingPops<S, T, P> f{pops + cstage * 18 * P + t + 1};
-            const Stencil<T> st{{rho + (0 * 4 + sm) * P, rho + (0 * 4 + sc) * P, rho + (0 * 4 + sp) * P},
-                                {rho + (1 * 4 + sm) * P, rho + (1 * 4 + sc) * P, rho + (1 * 4 + sp) * P},
+            const Stencil<T> st{{rho + sm * P, rho + sc * P, rho + sp * P},
                                 {msk + sm * P, msk + sc * P, msk + sp * P}, t + 1};
             const Nbr n = make_nbr(nx, x, xl, xr, yc, wrap1(yc - 1, ny), wrap1(yc + 1, ny));
             collide_push<S, T, FLAGS, true>(a, f, st, n); // 64-bit offsets: any lattice size

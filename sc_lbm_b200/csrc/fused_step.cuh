@@ -102,10 +102,23 @@ __device__ __forceinline__ float feq_dev(int i, float drho, float r, float ux, f
     return float(w_eq(i)) * fmaf(r, poly, drho);
 }
 
+// The two components' densities of one node side by side, so a stencil read
+// fetches both with one 8- (16-) byte shared-memory load.
+template <typename T> struct Vec2;
+template <> struct Vec2<float> {
+    using type = float2;
+    static __device__ __forceinline__ float2 make(float a, float b) { return make_float2(a, b); }
+};
+template <> struct Vec2<double> {
+    using type = double2;
+    static __device__ __forceinline__ double2 make(double a, double b) { return make_double2(a, b); }
+};
+template <typename T> using V2 = typename Vec2<T>::type;
+
 // Density/mask stencil around one node: rows below (0), at (1) and above (2)
-// the node, read at columns c-1, c, c+1.
+// the node, read at columns c-1, c, c+1; r[.][col] = (rho_0, rho_1).
 template <typename T> struct Stencil {
-    const T *r0[3], *r1[3];
+    const V2<T> *r[3];
     const uint8_t *m[3];
     int c;
 };
@@ -184,11 +197,13 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
         const int sl = cy(i) + 1;
         const int col = st.c + cx(i);
         nf[i] = SOLID ? st.m[sl][col] != 0 : true;
-        p0[i] = st.r0[sl][col];
-        p1[i] = st.r1[sl][col];
+        const V2<T> v = st.r[sl][col];
+        p0[i] = v.x;
+        p1[i] = v.y;
     }
     nf[0] = true;
-    const T psi0 = st.r0[1][st.c], psi1 = st.r1[1][st.c];
+    const V2<T> self = st.r[1][st.c];
+    const T psi0 = self.x, psi1 = self.y;
     if constexpr (EXACT) {
         // repulsive force, src/lbm.cpp:177-204
         // (selects, not branches: the sums take exactly the reference's terms)
@@ -350,7 +365,7 @@ constexpr int PF_DIST = 2;
 // nodes and issue no loads.  Same arithmetic as fused2_tile, same results.
 template <typename S, typename T, int TX, int FLAGS>
 __device__ __forceinline__ void fused2_tile_ahead(const Fused2Args<S, T> &a, const int xb,
-                                                  const int yb, T (&s_rho)[2][4][TX],
+                                                  const int yb, V2<T> (&s_rho)[4][TX],
                                                   uint8_t (&s_m)[4][TX])
 {
     constexpr bool SOLID = (FLAGS & KF_SOLID) != 0;
@@ -410,15 +425,13 @@ __device__ __forceinline__ void fused2_tile_ahead(const Fused2Args<S, T> &a, con
             if (SOLID && !m) rho[0] = rho[1] = T(0);
         }
         const int slot = (r + 1) & 3;
-        s_rho[0][slot][t] = rho[0];
-        s_rho[1][slot][t] = rho[1];
+        s_rho[slot][t] = Vec2<T>::make(rho[0], rho[1]);
         s_m[slot][t] = m;
         __syncthreads();
         if (r >= 1 && interior) {
             const int sc = r & 3, sm = (r - 1) & 3, sp = (r + 1) & 3;
             const int yc = wrap1(yb + r - 1, ny);
-            const Stencil<T> st{{s_rho[0][sm], s_rho[0][sc], s_rho[0][sp]},
-                                {s_rho[1][sm], s_rho[1][sc], s_rho[1][sp]},
+            const Stencil<T> st{{s_rho[sm], s_rho[sc], s_rho[sp]},
                                 {s_m[sm], s_m[sc], s_m[sp]}, t};
             const Nbr n = make_nbr(nx, x, xl, xr, yc, wrap1(yc - 1, ny), wrap1(yc + 1, ny));
             collide_push<S, T, FLAGS>(a, P, st, n);
@@ -470,7 +483,7 @@ template <typename S, typename T, int TX> struct CompactSmem {
 
 template <typename S, typename T, int TX, int FLAGS>
 __device__ __forceinline__ void fused2_tile_compact(const Fused2Args<S, T> &a, const int xb,
-                                                    const int yb, T (&s_rho)[2][4][TX],
+                                                    const int yb, V2<T> (&s_rho)[4][TX],
                                                     uint8_t (&s_m)[4][TX],
                                                     CompactSmem<S, T, TX> &cs, const bool down)
 {
@@ -527,8 +540,7 @@ __device__ __forceinline__ void fused2_tile_compact(const Fused2Args<S, T> &a, c
                     for (int i = 0; i < 9; ++i) Store<S>::st(a.fout[k] + elem<false>(i, a.N, node), T(0));
             }
         }
-        s_rho[0][slot][t] = rho[0];
-        s_rho[1][slot][t] = rho[1];
+        s_rho[slot][t] = Vec2<T>::make(rho[0], rho[1]);
         s_m[slot][t] = m;
         const bool work = interior && m && r >= 0 && r < nrow;
         if (work) {
@@ -563,8 +575,7 @@ __device__ __forceinline__ void fused2_tile_compact(const Fused2Args<S, T> &a, c
                 const int s_old = (q - 1) & 3, sc = q & 3, s_new = (q + 1) & 3;
                 const int sb = down ? s_new : s_old, sa = down ? s_old : s_new;
                 const int yc = wrap1(yb + phys(q - 1), ny);
-                const Stencil<T> st{{s_rho[0][sb], s_rho[0][sc], s_rho[0][sa]},
-                                    {s_rho[1][sb], s_rho[1][sc], s_rho[1][sa]},
+                const Stencil<T> st{{s_rho[sb], s_rho[sc], s_rho[sa]},
                                     {s_m[sb], s_m[sc], s_m[sa]}, col};
                 const Nbr n = make_nbr(nx, xc, wrap1(xc - 1, nx), wrap1(xc + 1, nx), yc,
                                        wrap1(yc - 1, ny), wrap1(yc + 1, ny));
@@ -585,7 +596,7 @@ __device__ __forceinline__ void fused2_tile_compact(const Fused2Args<S, T> &a, c
 template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS, bool PF = false,
           bool AHEAD = false, bool WIDE = false>
 __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int xb, const int yb,
-                                            T (&s_rho)[2][4][TX], uint8_t (&s_m)[4][TX],
+                                            V2<T> (&s_rho)[4][TX], uint8_t (&s_m)[4][TX],
                                             const bool down = false)
 {
     if constexpr (AHEAD && !TWO_PASS) {
@@ -665,8 +676,7 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
         } else {
             m = 0;
         }
-        s_rho[0][slot][t] = rho[0];
-        s_rho[1][slot][t] = rho[1];
+        s_rho[slot][t] = Vec2<T>::make(rho[0], rho[1]);
         s_m[slot][t] = m;
         __syncthreads();
 
@@ -675,8 +685,7 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
             const int s_old = (q - 1) & 3, sc = q & 3, s_new = (q + 1) & 3;
             const int sb = down ? s_new : s_old, sa = down ? s_old : s_new;
             const int yc = wrap1(yb + phys(q - 1), ny);
-            const Stencil<T> st{{s_rho[0][sb], s_rho[0][sc], s_rho[0][sa]},
-                                {s_rho[1][sb], s_rho[1][sc], s_rho[1][sa]},
+            const Stencil<T> st{{s_rho[sb], s_rho[sc], s_rho[sa]},
                                 {s_m[sb], s_m[sc], s_m[sa]}, t};
             const Nbr n = make_nbr(nx, x, xl, xr, yc, wrap1(yc - 1, ny), wrap1(yc + 1, ny));
             collide_push<S, T, FLAGS, WIDE>(a, prev, st, n);
@@ -708,7 +717,7 @@ template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS, bool PF = fa
 __global__ void __launch_bounds__(TX, (fused_min_ctas<T, AHEAD>()))
     k_fused2(const __grid_constant__ Fused2Args<S, T> a)
 {
-    __shared__ T s_rho[2][4][TX];
+    __shared__ V2<T> s_rho[4][TX];
     __shared__ uint8_t s_m[4][TX];
     if constexpr (COMPACT && (FLAGS & KF_SOLID) != 0 && !TWO_PASS) {
         __shared__ CompactSmem<S, T, TX> cs;

@@ -84,6 +84,17 @@ int sclbm_geometry_add_array_spacing(sclbm_geometry *g, const size_t *props, siz
 int sclbm_geometry_add_array_numbers(sclbm_geometry *g, const size_t *props, size_t nprops,
                                      const size_t bounds[4], size_t nobj_x, size_t nobj_y,
                                      const char *type);
+/* Seeded porous medium: non-overlapping disks (add_circle, D = 2r + 1, r in
+ * [rmin, rmax]) placed by random sequential addition with a one-node gap
+ * until the fluid fraction reaches `porosity`, or max_tries draws were made,
+ * or max_misses draws in a row found no room; disk centres keep wall_rows
+ * rows clear of the top and bottom.  Existing solid nodes count as occupied.
+ * The draws are the splitmix64 stream of sc_lbm_b200/workloads.py, so a seed
+ * gives the same medium as its disk_mask.  No reference counterpart (the
+ * reference's drivers place objects by hand or in regular arrays). */
+int sclbm_geometry_add_random_disks(sclbm_geometry *g, double porosity, int rmin, int rmax,
+                                    uint64_t seed, int wall_rows, long max_tries, long max_misses,
+                                    size_t *placed);
 /* Geometry::set_node_fluid / set_node_solid, include/geometry.h:200-210 */
 int sclbm_geometry_set_node(sclbm_geometry *g, size_t x, size_t y, int fluid);
 /* Geometry::get_geom, include/geometry.h:262 (count must be nx*ny) */

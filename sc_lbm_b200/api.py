@@ -88,6 +88,14 @@ class Geometry(_Handle):
             call("sclbm_geometry_add_array_spacing", self._h, P, len(props), B, a, b,
                  object_type.encode())
 
+    def add_random_disks(self, porosity, rmin, rmax, seed, wall_rows=0, max_tries=20000,
+                         max_misses=300) -> int:
+        """Seeded non-overlapping disks to the given fluid fraction (native)."""
+        n = C.c_size_t()
+        call("sclbm_geometry_add_random_disks", self._h, float(porosity), int(rmin), int(rmax),
+             int(seed), int(wall_rows), int(max_tries), int(max_misses), C.byref(n))
+        return n.value
+
     def set_node_fluid(self, x, y):
         call("sclbm_geometry_set_node", self._h, x, y, 1)
 

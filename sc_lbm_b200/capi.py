@@ -135,6 +135,9 @@ SIGNATURES = {
                                                _SZ, _SZ, _SZ, _SZ, _D]),
     "sclbm_domain_velocity_stats": (C.c_int, [_VP, C.c_int, _D]),
     "sclbm_domain_profile": (C.c_int, [_VP, C.c_int, C.c_int, _D, _SZ]),
+    "sclbm_geometry_add_random_disks": (C.c_int, [_VP, C.c_double, C.c_int, C.c_int, C.c_uint64,
+                                                  C.c_int, C.c_long, C.c_long,
+                                                  C.POINTER(_SZ)]),
     "sclbm_tuned_config": (C.c_int, [_SZ, _SZ, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                      C.POINTER(C.c_int)]),
 }

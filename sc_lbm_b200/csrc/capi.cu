@@ -205,6 +205,86 @@ int sclbm_geometry_add_circle(sclbm_geometry *g, size_t D, size_t xc, size_t yc)
     g->dirty = true;
     return geom_add_object(g->mask, g->nx, g->ny, 3, D, D, xc, yc);
 }
+// Seeded random sequential addition of non-overlapping disks (the porous media
+// of the drainage and ensemble configurations): draws from the splitmix64
+// stream u_k = splitmix(seed, k) exactly as sc_lbm_b200/workloads.py's
+// Stream/disk_mask do, keeps a one-node gap (occupancy window of radius
+// r + 1.5), stops at the target solid fraction, after max_tries draws or after
+// max_misses failed draws in a row, then adds the disks with add_circle
+// (D = 2r + 1).  The existing solid nodes (walls) count as occupied.
+namespace {
+inline double splitmix_u01_host(uint64_t seed, uint64_t k)
+{
+    uint64_t z = k + seed * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z = z ^ (z >> 31);
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+} // namespace
+
+int sclbm_geometry_add_random_disks(sclbm_geometry *g, double porosity, int rmin, int rmax,
+                                    uint64_t seed, int wall_rows, long max_tries, long max_misses,
+                                    size_t *placed)
+{
+    CHECK_NULL(g);
+    if (rmin < 0 || rmax < rmin || !(porosity >= 0.0 && porosity <= 1.0) || wall_rows < 0)
+        return set_error(SCLBM_E_INVALID_ARGUMENT, "bad disk parameters");
+    const long nx = (long)g->nx, ny = (long)g->ny;
+    std::vector<uint8_t> occ(g->mask.size());
+    double solid = 0.0;
+    long nsolid = 0;
+    for (size_t i = 0; i < occ.size(); ++i) {
+        occ[i] = g->mask[i] == 0;
+        nsolid += occ[i];
+    }
+    solid = (double)nsolid;
+    uint64_t k = 0;
+    auto integer = [&](long lo, long hi) {
+        const double u = splitmix_u01_host(seed, k++);
+        const long n = (long)(u * (double)(hi - lo + 1)); // truncation toward zero
+        return lo + std::min(hi - lo, n);
+    };
+    const double target = (1.0 - porosity) * (double)nx * (double)ny;
+    std::vector<long> disks;
+    long tries = 0, misses = 0;
+    while (solid < target && tries < max_tries && misses < max_misses) {
+        ++tries;
+        ++misses;
+        const long r = integer(rmin, rmax);
+        const long xc = integer(r, nx - 1 - r);
+        const long yc = integer(r + wall_rows, ny - 1 - r - wall_rows);
+        if (xc - r < 0 || yc - r < 0 || xc + r >= nx || yc + r >= ny) continue;
+        const long y0 = std::max(0L, yc - r - 1), y1 = std::min(ny, yc + r + 2);
+        const long x0 = std::max(0L, xc - r - 1), x1 = std::min(nx, xc + r + 2);
+        const double lim = ((double)r + 1.5) * ((double)r + 1.5);
+        bool hit = false;
+        for (long y = y0; y < y1 && !hit; ++y)
+            for (long x = x0; x < x1; ++x)
+                if ((double)((y - yc) * (y - yc) + (x - xc) * (x - xc)) <= lim && occ[y * nx + x]) {
+                    hit = true;
+                    break;
+                }
+        if (hit) continue;
+        for (long y = y0; y < y1; ++y)
+            for (long x = x0; x < x1; ++x)
+                if ((double)((y - yc) * (y - yc) + (x - xc) * (x - xc)) <= lim) occ[y * nx + x] = 1;
+        misses = 0;
+        disks.push_back(r);
+        disks.push_back(xc);
+        disks.push_back(yc);
+        solid += M_PI * (((double)r + 0.5) * ((double)r + 0.5));
+    }
+    g->dirty = true;
+    for (size_t i = 0; i < disks.size(); i += 3) {
+        const int rc = geom_add_object(g->mask, g->nx, g->ny, 3, 2 * disks[i] + 1, 2 * disks[i] + 1,
+                                       disks[i + 1], disks[i + 2]);
+        if (rc) return rc;
+    }
+    if (placed) *placed = disks.size() / 3;
+    return SCLBM_OK;
+}
+
 int sclbm_geometry_add_array_spacing(sclbm_geometry *g, const size_t *props, size_t nprops,
                                      const size_t bounds[4], size_t dx, size_t dy,
                                      const char *type)

@@ -83,44 +83,20 @@ def populations(rho: np.ndarray, mask=None) -> np.ndarray:
 def disk_mask(nx: int, ny: int, porosity: float, rmin: int, rmax: int, seed: int,
               walls: str | None = None, max_tries: int = 20000, max_misses: int = 300):
     """Non-overlapping disks (add_circle with D = 2r + 1, placed inside the
-    bounds the reference's check_object_bounds accepts) added in seeded random
-    order until the fluid fraction drops to `porosity`, or `max_tries` draws
-    were made, or `max_misses` draws in a row found no room (jammed).  The
-    final mask is built by the library's Geometry (the reference's mask rules).  Returns (mask int32 [ny*nx], disks [(D, xc, yc)], porosity)."""
+    bounds the reference's check_object_bounds accepts, one node apart) added
+    in seeded random order until the fluid fraction drops to `porosity`, or
+    `max_tries` draws were made, or `max_misses` draws in a row found no room
+    (jammed).  Runs in the library (sclbm_geometry_add_random_disks) on a
+    Geometry with the walls, so the mask follows the reference's rules.
+    Returns (mask int32 [ny*nx], number of disks, fluid fraction)."""
     from .api import Geometry
-    s = Stream(seed)
-    occ = np.zeros((ny, nx), dtype=bool)
-    wall_rows = 0
-    if walls == "x":
-        occ[0, :] = occ[-1, :] = True
-        wall_rows = 1
-    yy, xx = np.mgrid[0:ny, 0:nx]
-    disks, solid, tries, misses = [], occ.sum(), 0, 0
-    target = (1.0 - porosity) * nx * ny
-    while solid < target and tries < max_tries and misses < max_misses:
-        tries += 1
-        misses += 1
-        r = s.integer(rmin, rmax)
-        D = 2 * r + 1
-        xc = s.integer(r, nx - 1 - r)
-        yc = s.integer(r + wall_rows, ny - 1 - r - wall_rows)
-        if xc - r < 0 or yc - r < 0 or xc + r >= nx or yc + r >= ny:
-            continue
-        y0, y1, x0, x1 = max(0, yc - r - 1), min(ny, yc + r + 2), max(0, xc - r - 1), min(nx, xc + r + 2)
-        win = (yy[y0:y1, x0:x1] - yc) ** 2 + (xx[y0:y1, x0:x1] - xc) ** 2 <= (r + 1.5) ** 2
-        if np.any(occ[y0:y1, x0:x1] & win):
-            continue
-        occ[y0:y1, x0:x1] |= win
-        misses = 0
-        disks.append((D, xc, yc))
-        solid += np.pi * (r + 0.5) ** 2
     g = Geometry(nx, ny)
     if walls:
         g.add_walls(1, walls)
-    for D, xc, yc in disks:
-        g.add_circle(D, xc, yc)
+    n = g.add_random_disks(porosity, rmin, rmax, seed, wall_rows=1 if walls == "x" else 0,
+                           max_tries=max_tries, max_misses=max_misses)
     m = g.get_geom()
-    return m, disks, float(m.mean())
+    return m, n, float(m.mean())
 
 
 # ----------------------------------------------------------------------------- configs
@@ -151,7 +127,7 @@ def drainage(nx: int = 2048, ny: int = 1024, seed: int = 11, porosity: float = 0
     r2 = np.where(left, 0.06, 2.0)
     return dict(nx=nx, ny=ny, mask=m, tau=(1.0, 1.0), G=0.9, Gs=(-0.2, 0.2),
                 force1=force_vec(1e-5, "x"), f1=populations(r1, m), f2=populations(r2, m),
-                porosity=phi, disks=len(disks))
+                porosity=phi, disks=disks)
 
 
 def spinodal(nx: int, ny: int, seed: int = 101, amp: float = 0.01):

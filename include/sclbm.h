@@ -349,6 +349,19 @@ int sclbm_domain_velocity_stats(sclbm_domain *d, int comp, double out[3]);
  * nodes of row y (0 for a row without fluid); count must be ny.  The channel
  * profile compared with scripts/benchmark_utils.py:8-52. */
 int sclbm_domain_profile(sclbm_domain *d, int comp, int axis, double *prof, size_t count);
+/* Contact angle of a droplet (component 1 - bulk) resting on a flat solid,
+ * as benchmarks/two_phase_two_components_flows/contact_angles/
+ * compute_contact_angles.py:45-106 measures it from the density files: the
+ * band rho_b - rho_d <= 0, rho_d <= rho_bulk, rho_b > rho_disp; the smallest
+ * and largest x of its two lowest rows extrapolated half a node below the
+ * lowest row give the base ends xL (out[4]) and xR (out[5]), L = xR - xL
+ * (out[1]); H = row extent + 0.5 (out[2]); R = (4 H^2 + L^2) / (8 H)
+ * (out[3]); out[0] = atan(L / (2 (R - H))) in degrees, in [0, 180).
+ * out[6], out[7] = lowest and highest band row, out[8] = band nodes.
+ * SCLBM_E_OUT_OF_RANGE when the band is empty or its lowest row is the only
+ * one (the script's reductions over empty arrays). */
+int sclbm_domain_contact_angle(sclbm_domain *d, int bulk, double rho_bulk, double rho_disp,
+                               double out[9]);
 
 /* ------------------------------------------------------------------- batch
  * Many independent domains of one precision advanced together: one launch

@@ -1,0 +1,62 @@
+"""numpy restatements of the reference's post-processing scripts (TEST
+INFRASTRUCTURE ONLY): the checkers of the library's on-device measurements.
+
+* ``contact_angle`` -- benchmarks/two_phase_two_components_flows/
+  contact_angles/compute_contact_angles.py:45-106, on density fields held in
+  memory instead of the loaded text files.
+
+Pinned against the script itself: tests/golden/make_contact_angle_golden.py
+runs the unmodified script on seeded synthetic fields and records what it
+prints (tests/golden/contact_angle_golden.json).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def contact_angle(rho_b: np.ndarray, rho_d: np.ndarray, nx: int, ny: int,
+                  rho_bulk: float = 2.0, rho_disp: float = 0.06) -> dict:
+    """Contact angle of the droplet (density rho_d) on a flat solid below it.
+
+    The interface band (compute_contact_angles.py:46) is rho_b - rho_d <= 0,
+    rho_d <= rho_bulk, rho_b > rho_disp.  Its lowest row y2 and the row above,
+    y1 (:48-55), give each end of the base: the smallest (left) and largest
+    (right) x on both rows, one node apart at least (:62-79), extended by the
+    line through them to half a node below the lowest row (:72-90).  The cap
+    height is the band's row extent + 0.5 (:96), its radius
+    R = (4H^2 + L^2) / (8H) (:99) and the angle atan(L / (2(R - H))) in
+    degrees, moved into [0, 180) (:102-106).  Raises ValueError on an empty
+    band or a band of one row, where the script's reductions fail.
+    """
+    rb = np.asarray(rho_b, dtype=np.float64).reshape(ny, nx)
+    rd = np.asarray(rho_d, dtype=np.float64).reshape(ny, nx)
+    ys, xs = np.where((rb - rd <= 0) & (rd <= rho_bulk) & (rb > rho_disp))
+    if ys.size == 0:
+        raise ValueError("no interface nodes")
+    y2 = int(ys.min())
+    y1 = y2 + 1
+    row2, row1 = xs[ys == y2], xs[ys == y1]
+    if row1.size == 0:
+        raise ValueError("no interface nodes above the lowest row")
+    xL1, xL2 = float(row1.min()), float(row2.min())
+    xR1, xR2 = float(row1.max()), float(row2.max())
+    y_base = y2 - 0.5
+    if xL1 == xL2:
+        xL1 -= 1
+    if xR1 == xR2:
+        xR1 -= 1
+    slope_l = (y1 - y2) / (xL1 - xL2)
+    slope_r = (y1 - y2) / (xR1 - xR2)
+    inter_l = y2 - slope_l * xL2
+    inter_r = y2 - slope_r * xR2
+    xL = 1 / slope_l * (y_base - inter_l)
+    xR = 1 / slope_r * (y_base - inter_r)
+    L = xR - xL
+    H = float(ys.max() - ys.min()) + 0.5
+    R = (4 * H * H + L * L) / (8 * H)
+    with np.errstate(divide="ignore"):
+        theta = float(np.degrees(np.arctan(np.float64(L) / (2 * (R - H)))))
+    if theta < 0:
+        theta += 180
+    return {"theta": theta, "L": L, "H": H, "R": R, "xL": xL, "xR": xR, "y_min": y2,
+            "y_max": int(ys.max()), "band_nodes": int(ys.size)}

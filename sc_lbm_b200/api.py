@@ -341,6 +341,16 @@ class Domain(_Handle):
         call("sclbm_domain_profile", self._h, int(comp), int(axis), _dp(out), self.ny)
         return out
 
+    def contact_angle(self, bulk, rho_bulk=2.0, rho_disp=0.06) -> dict:
+        """Contact angle of the droplet (the other component) on a flat solid,
+        measured as compute_contact_angles.py does (degrees)."""
+        out = np.zeros(9)
+        call("sclbm_domain_contact_angle", self._h, int(bulk), float(rho_bulk), float(rho_disp),
+             _dp(out))
+        return {"theta": out[0], "L": out[1], "H": out[2], "R": out[3], "xL": out[4],
+                "xR": out[5], "y_min": int(out[6]), "y_max": int(out[7]),
+                "band_nodes": int(out[8])}
+
     def run(self, f1, f2, nsteps, rho1, rho2=None):
         call("sclbm_domain_run", self._h, _dp(f1), None if f2 is None else _dp(f2), int(nsteps),
              _dp(rho1), None if rho2 is None else _dp(rho2))

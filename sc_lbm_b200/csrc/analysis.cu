@@ -13,12 +13,18 @@
 //    scripts/benchmark_utils.py:55-63);
 //  * the row profile of u_x (mean over each row's fluid nodes), the quantity
 //    a channel flow is compared with the analytic parabola on
-//    (scripts/benchmark_utils.py:8-52).
+//    (scripts/benchmark_utils.py:8-52);
+//  * the contact angle of a droplet resting on a flat solid
+//    (benchmarks/two_phase_two_components_flows/contact_angles/
+//    compute_contact_angles.py:45-106): the base from the two lowest rows of
+//    the droplet-side interface band, the height from its row extent, and the
+//    angle of the circular cap through them.
 //
 // Densities and velocities are the FP64 values of Fluid::compute_density /
 // compute_velocities (shifted forms add w_i rho_ref back); every reduction is
 // deterministic (integer atomics on indices and on the bit patterns of
 // non-negative doubles, fixed-order block sums).
+#include <cmath>
 #include <cstring>
 #include <type_traits>
 #include <vector>
@@ -86,6 +92,38 @@ __global__ void k_laplace(size_t N, int nx, const uint8_t *__restrict__ mask, co
             atomicMax(&out->ymax, y);
             atomicMin(&out->xmin, x);
             atomicMax(&out->xmax, x);
+            atomicAdd(&out->band, 1ull);
+        }
+    }
+}
+
+// Contact-angle band (compute_contact_angles.py:46): nodes with
+// rho_b - rho_d <= 0, rho_d <= rho_bulk and rho_b > rho_disp; per row the
+// smallest and largest x of the band, and its first and last rows.
+struct ContactOut {
+    unsigned int ymin, ymax;
+    unsigned long long band;
+};
+
+template <typename S>
+__global__ void k_contact_band(size_t N, int nx, const uint8_t *__restrict__ mask,
+                               const S *__restrict__ fb, const S *__restrict__ fd, double rrb,
+                               double rrd, int shifted, double rho_bulk, double rho_disp,
+                               unsigned int *__restrict__ row_xmin, unsigned int *__restrict__ row_xmax,
+                               ContactOut *out)
+{
+    for (size_t n = blockIdx.x * (size_t)blockDim.x + threadIdx.x; n < N;
+         n += (size_t)gridDim.x * blockDim.x) {
+        double rb, rd, jx, jy;
+        moments(fb, N, n, rrb, shifted, rb, jx, jy);
+        moments(fd, N, n, rrd, shifted, rd, jx, jy);
+        if (!mask[n]) rb = rd = 0.0;
+        if (rb - rd <= 0.0 && rd <= rho_bulk && rb > rho_disp) {
+            const unsigned int y = (unsigned int)(n / nx), x = (unsigned int)(n % nx);
+            atomicMin(&row_xmin[y], x);
+            atomicMax(&row_xmax[y], x);
+            atomicMin(&out->ymin, y);
+            atomicMax(&out->ymax, y);
             atomicAdd(&out->band, 1ull);
         }
     }
@@ -212,6 +250,76 @@ extern "C" int sclbm_domain_laplace_measure(sclbm_domain *d, int bulk, double G,
     out[2] = Rr;
     out[3] = Rc;
     out[4] = (double)h.band;
+    return SCLBM_OK;
+}
+
+extern "C" int sclbm_domain_contact_angle(sclbm_domain *d, int bulk, double rho_bulk,
+                                          double rho_disp, double out[9])
+{
+    if (!d || !out) return set_error(SCLBM_E_INVALID_ARGUMENT, "null argument");
+    if (d->ncomp != 2 || (bulk != 0 && bulk != 1))
+        return set_error(SCLBM_E_INVALID_ARGUMENT, "a two-component domain and bulk = 0 or 1");
+    const size_t ny = d->ny;
+    ContactOut h{0xffffffffu, 0u, 0ull};
+    ContactOut *dv = nullptr;
+    unsigned int *rows = nullptr; // [0, ny): smallest x per row, [ny, 2 ny): largest
+    SCLBM_CUDA(cudaMalloc(&dv, sizeof(ContactOut)));
+    cudaError_t e = cudaMalloc(&rows, 2 * ny * sizeof(unsigned int));
+    if (e != cudaSuccess) {
+        cudaFree(dv);
+        return cuda_fail(e, "contact angle scratch");
+    }
+    cudaStream_t s = stream();
+    e = cudaMemcpyAsync(dv, &h, sizeof h, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(rows, 0xff, ny * sizeof(unsigned int), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(rows + ny, 0, ny * sizeof(unsigned int), s);
+    const int drop = 1 - bulk;
+    const bool shifted = d->prec != SCLBM_FP64;
+    if (e == cudaSuccess) {
+        with_precision(d, [&](auto tag) {
+            using S = std::remove_const_t<std::remove_pointer_t<decltype(tag)>>;
+            k_contact_band<S><<<STAT_BLOCKS, 256, 0, s>>>(
+                d->N, (int)d->nx, d->d_mask, (const S *)d->buf[d->parity][bulk],
+                (const S *)d->buf[d->parity][drop], d->p.rho_ref[bulk], d->p.rho_ref[drop],
+                shifted ? 1 : 0, rho_bulk, rho_disp, rows, rows + ny, dv);
+        });
+        e = cudaGetLastError();
+    }
+    std::vector<unsigned int> hr(2 * ny);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, dv, sizeof h, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(hr.data(), rows, 2 * ny * sizeof(unsigned int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(dv);
+    cudaFree(rows);
+    if (e != cudaSuccess) return cuda_fail(e, "contact angle");
+    if (h.band == 0) return set_error(SCLBM_E_OUT_OF_RANGE, "contact angle: no interface nodes");
+    // compute_contact_angles.py:48-106: the two lowest rows of the band give
+    // each end of the base, extrapolated half a node below the lowest row
+    const size_t y2 = h.ymin, y1 = y2 + 1;
+    if (y1 >= ny || hr[y1] == 0xffffffffu)
+        return set_error(SCLBM_E_OUT_OF_RANGE, "contact angle: no interface nodes above the lowest row");
+    double xL1 = hr[y1], xL2 = hr[y2], xR1 = hr[ny + y1], xR2 = hr[ny + y2];
+    const double yA = (double)y1, yB = (double)y2, yBase = (double)h.ymin - 0.5;
+    if (xL1 == xL2) xL1 = xL1 - 1;
+    if (xR1 == xR2) xR1 = xR1 - 1;
+    const double slopeL = (yA - yB) / (xL1 - xL2), slopeR = (yA - yB) / (xR1 - xR2);
+    const double interL = yB - slopeL * xL2, interR = yB - slopeR * xR2;
+    const double xL = 1 / slopeL * (yBase - interL), xR = 1 / slopeR * (yBase - interR);
+    const double L = xR - xL;
+    const double H = (double)(h.ymax - h.ymin) + 0.5;
+    const double R = (4 * H * H + L * L) / (8 * H);
+    double theta = std::atan(L / (2 * (R - H))) * (180.0 / 3.141592653589793);
+    if (theta < 0) theta += 180;
+    out[0] = theta;
+    out[1] = L;
+    out[2] = H;
+    out[3] = R;
+    out[4] = xL;
+    out[5] = xR;
+    out[6] = (double)h.ymin;
+    out[7] = (double)h.ymax;
+    out[8] = (double)h.band;
     return SCLBM_OK;
 }
 

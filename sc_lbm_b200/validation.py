@@ -1,7 +1,7 @@
 """Full-size runs of the sc_lbm configurations on one B200 (physics and
 throughput checks beyond the benchmark line).
 
-    python -m sc_lbm_b200.validation [poiseuille laplace drainage ensemble spinodal]
+    python -m sc_lbm_b200.validation [poiseuille laplace drainage ensemble spinodal contact]
                                      [--out results.json] [--quick]
 
 Each run prints one JSON object; ``--out`` collects them.  The FP64 GPU form is
@@ -23,6 +23,10 @@ shifted forms.  Inputs are seeded (sc_lbm_b200/workloads.py).
 * spinodal   -- 16384 x 8192 periodic, FP64 / FP32 / FP16, 5,000 steps:
   MLUPS, fraction of the measured HBM bandwidth, density error and mass drift
   against FP64.
+* contact    -- the reference's contact-angle benchmark: 400 x 306, a droplet
+  on a solid shelf for eight solid interaction parameters in one batch, FP64
+  and FP32-shifted, 30,000 steps: the angle measured on the device
+  (compute_contact_angles.py's construction) against the parameter.
 """
 from __future__ import annotations
 
@@ -310,8 +314,54 @@ def spinodal(args):
     return out
 
 
+def contact(args):
+    """The reference's contact-angle benchmark (contact_angles.cpp): one
+    400 x 306 domain per solid interaction parameter, all in one batch, and
+    the angle measured on the device as compute_contact_angles.py measures it
+    from the density files."""
+    torch, sc, W, stream = _env()
+    gs_values = [-0.4, -0.3, -0.2, -0.1, 0.1, 0.2, 0.3, 0.4]
+    steps = 5000 if args.quick else 30000
+    out = {"config": "contact angles 400x306, droplet on a 341x20 shelf, G=0.9, "
+                     "Gs_droplet -0.4..0.4, one batch per precision", "steps": steps}
+    for prec, name in ((sc.FP64, "fp64"), (sc.FP32_SHIFTED, "fp32s")):
+        ws = [W.contact_angle(g) for g in gs_values]
+        doms = []
+        for w in ws:
+            fl = np.asarray(w["mask"]).ravel() != 0
+            rr = tuple(float(w[k].reshape(9, -1).sum(0)[fl].mean()) for k in ("f1", "f2"))
+            d = sc.Domain(w["nx"], w["ny"], w["mask"], W.params_of(w, sc, rho_ref=rr), prec)
+            d.upload_f(0, w["f1"])
+            d.upload_f(1, w["f2"])
+            doms.append(d)
+        m0 = [d.mass_momentum() for d in doms]
+        b = sc.Batch(doms)
+        ms = _timed(torch, stream, lambda: b.step(steps))
+        rows = []
+        for g, d, a in zip(gs_values, doms, m0):
+            row = {"gs_droplet": g}
+            try:
+                row.update(d.contact_angle(0, rho_bulk=2.0, rho_disp=0.06))
+            except IndexError as e:
+                row["error"] = str(e)
+            m1 = d.mass_momentum()
+            row["mass_drift"] = [float((m1[3 * c] - a[3 * c]) / a[3 * c]) for c in range(2)]
+            rows.append(row)
+        th = [r.get("theta") for r in rows]
+        out[name] = {"angles": rows, "theta_deg": th,
+                     "monotonic_in_gs": all(x is not None for x in th) and
+                     all(th[i] < th[i + 1] for i in range(len(th) - 1)),
+                     "ms": round(ms, 2),
+                     "mlups": round(sum(d.N for d in doms) * steps / (ms * 1e-3) / 1e6, 1)}
+        del b, doms
+    a, b_ = out["fp64"]["theta_deg"], out["fp32s"]["theta_deg"]
+    out["max_abs_theta_diff_fp32s_deg"] = max(
+        (abs(x - y) for x, y in zip(a, b_) if x is not None and y is not None), default=None)
+    return out
+
+
 RUNS = {"poiseuille": poiseuille, "laplace": laplace, "drainage": drainage,
-        "ensemble": ensemble, "spinodal": spinodal}
+        "ensemble": ensemble, "spinodal": spinodal, "contact": contact}
 
 
 def main():

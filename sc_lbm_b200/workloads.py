@@ -22,6 +22,8 @@ drivers, scaled as the project's measurement plan states):
   Gs in [-0.3, 0.3], tau in [0.6, 1.5];
 * ``spinodal``    -- periodic, tau = 1, G = 1.2, rho = 1 +- 1% per component
   (phase_separation.cpp:57-116).
+* ``contact_angle`` -- 400 x 306, a droplet on a solid shelf, one solid
+  interaction parameter per domain (contact_angles.cpp:39-109).
 """
 from __future__ import annotations
 
@@ -128,6 +130,26 @@ def drainage(nx: int = 2048, ny: int = 1024, seed: int = 11, porosity: float = 0
     return dict(nx=nx, ny=ny, mask=m, tau=(1.0, 1.0), G=0.9, Gs=(-0.2, 0.2),
                 force1=force_vec(1e-5, "x"), f1=populations(r1, m), f2=populations(r2, m),
                 porosity=phi, disks=disks)
+
+
+def contact_angle(gs_droplet: float, nx: int = 400, ny: int = 306):
+    """A droplet on a solid shelf (contact_angles.cpp:39-109): the rectangle
+    341 x 20 around (199, 152) is solid; component 1 (the bulk, Gs = -gs) at
+    rho 2.0 with 0.06 of component 2 (the droplet, Gs = +gs), except the
+    square of half-width 30 around (199, 192), which holds the reverse
+    (initialize_fluid_rectangle, src/lbm.cpp:51-99: nodes xc - 29 .. xc + 29,
+    yc - 29 .. yc + 29).  G = 0.9, tau = 1, no volume force."""
+    from .api import Geometry
+    g = Geometry(nx, ny)
+    g.add_rectangle(341, 20, 199, 152)
+    m = g.get_geom()
+    N = nx * ny
+    yy, xx = np.divmod(np.arange(N), nx)
+    sq = (xx >= 199 - 30 + 1) & (xx <= 199 + 30 - 1) & (yy >= 192 - 30 + 1) & (yy <= 192 + 30 - 1)
+    r1 = np.where(sq, 0.06, 2.0)
+    r2 = np.where(sq, 2.0, 0.06)
+    return dict(nx=nx, ny=ny, mask=m, tau=(1.0, 1.0), G=0.9, Gs=(-gs_droplet, gs_droplet),
+                f1=populations(r1, m), f2=populations(r2, m), gs_droplet=gs_droplet)
 
 
 def spinodal(nx: int, ny: int, seed: int = 101, amp: float = 0.01):

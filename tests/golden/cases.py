@@ -189,6 +189,12 @@ def two_cases() -> dict:
                               fluid1=(1.0, 0.9, -0.294), fluid2=(1.0, 0.9, 0.294),
                               init=("rectangle", 2.0, 2.0, 0.06, 0.06, 40, 16, 14, 15),
                               force=(3, force_vec(1e-4, "x")), steps=100)
+    # droplet on a solid shelf (contact_angles.cpp:39-137, reduced): periodic,
+    # rectangle initialiser, solid interaction -0.2 / +0.2, no volume force
+    c["contact_120x90"] = dict(nx=120, ny=90, geom=[("rectangle", 101, 8, 59, 30)], mode="two",
+                               fluid1=(1.0, 0.9, 0.2), fluid2=(1.0, 0.9, -0.2),
+                               init=("rectangle", 2.0, 2.0, 0.06, 0.06, 59, 50, 14, 14),
+                               force=(0, [0.0] * 9), steps=2000)
     # a component absent from part of the lattice (rho = 0 keeps the previous u_eq)
     nx, ny = 24, 16
     f1 = noisy_f(41, nx, ny, 1.0, 0.01).reshape(9, -1)

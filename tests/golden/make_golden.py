@@ -1,6 +1,6 @@
 """Generate the golden fixtures from the compiled reference (oracle/_ref).
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]
 
 For every case of tests/golden/cases.py it runs the unmodified reference
 library (LBMFluids/sc_lbm compiled from its own sources by oracle/Makefile,
@@ -34,10 +34,20 @@ def digest(a: np.ndarray) -> str:
 
 
 def main() -> None:
+    """All cases, or only those named on the command line (the digests of the
+    others are kept from the committed fixture)."""
     if not pyoracle.have_ref():
         pyoracle.build(ref=True)
+    names = sys.argv[1:]
     out, arrays = {}, {}
+    if names:
+        with open(os.path.join(HERE, "golden_digests.json")) as fh:
+            out = json.load(fh)["cases"]
+        with np.load(os.path.join(HERE, "golden_arrays.npz")) as z:
+            arrays = {k: z[k] for k in z.files}
     for name, case in list(cases.all_cases().items()) + list(cases.long_cases().items()):
+        if names and name not in names:
+            continue
         res = pyoracle.run_ref(case)
         out[name] = {k: [digest(v), int(v.size)] for k, v in sorted(res.items())}
         if name in cases.FULL_ARRAY_CASES:

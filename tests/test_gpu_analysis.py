@@ -7,7 +7,10 @@ post-processing done in numpy on the downloaded fields.
   largest |u| identical, the mean of the nonzero |u| to summation order;
 * the channel profile (row means of u_x) against numpy and, after 10,000
   steps of the 200 x 50 Poiseuille channel, against the analytic parabola of
-  scripts/benchmark_utils.py:8-52.
+  scripts/benchmark_utils.py:8-52;
+* the contact angle (compute_contact_angles.py:45-106) against the numpy
+  restatement in oracle/post.py and the angles the reference's script printed
+  on the same fields.
 """
 import numpy as np
 import pytest
@@ -92,3 +95,78 @@ def test_poiseuille_profile_against_analytic(sclbm):
     ua = w["g"] * h * h / (2 * mu) * (1 - (lat / h) ** 2)
     assert np.linalg.norm(prof[1:-1] - ua) / np.linalg.norm(ua) < 5e-3
     assert prof[0] == 0.0 and prof[-1] == 0.0
+
+
+def _contact_golden():
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "contact_angle_golden.json")) as fh:
+        return json.load(fh)["theta_deg"]
+
+
+@pytest.mark.parametrize("prec_name", ["FP64", "FP32_SHIFTED", "FP16_SHIFTED"])
+def test_contact_angle_against_reference_script(sclbm, prec_name):
+    """The device measurement on the synthetic fields the reference's own
+    script was run on (contact_angle_golden.json): every quantity equal to
+    the numpy restatement on the downloaded densities, and the angle equal to
+    the one the script printed."""
+    import contact_fields
+    from oracle import post
+    from sc_lbm_b200 import workloads as W
+    golden = _contact_golden()
+    for key in contact_fields.CASES:
+        rb, rd = contact_fields.fields(key)
+        ny, nx = rb.shape
+        mask = ((rb != 0) | (rd != 0)).astype(np.int32).ravel()
+        rr = (float(rb[rb > 0].mean()), float(rd[rd > 0].mean()))
+        d = sclbm.Domain(nx, ny, mask, sclbm.make_params(ncomp=2, rho_ref=rr),
+                         getattr(sclbm, prec_name))
+        d.upload_f(0, W.populations(rb.ravel(), mask))
+        d.upload_f(1, W.populations(rd.ravel(), mask))
+        got = d.contact_angle(0, rho_bulk=2.0, rho_disp=0.06)
+        want = post.contact_angle(d.download_rho(0), d.download_rho(1), nx, ny, 2.0, 0.06)
+        # the shifted forms' densities carry their storage rounding (core nodes
+        # at rho_b = 0.06 may join the band); the band's ends and rows do not move
+        keys = ("L", "H", "R", "xL", "xR", "y_min", "y_max")
+        for k in keys + (("band_nodes",) if prec_name == "FP64" else ()):
+            assert got[k] == want[k], (key, k)
+        assert got["theta"] == pytest.approx(want["theta"], rel=1e-14, abs=1e-12)
+        assert got["theta"] == pytest.approx(golden[key], rel=1e-14, abs=1e-12), key
+
+
+def test_contact_angle_reduced_benchmark(sclbm):
+    """A droplet on a shelf after 2,000 FP64 steps (the reduced contact-angle
+    case, bit-identical to the compiled reference): the device measurement
+    equals the restatement on the reference's own final densities."""
+    import cases
+    import gpu_runner
+    from oracle import post
+    case = cases.all_cases()["contact_120x90"]
+    d = gpu_runner.make_domain(sclbm, case, sclbm.FP64)
+    d.step(case["steps"])
+    got = d.contact_angle(0, rho_bulk=2.0, rho_disp=0.06)
+    want = post.contact_angle(d.download_rho(0), d.download_rho(1), 120, 90, 2.0, 0.06)
+    for k in ("L", "H", "R", "xL", "xR", "y_min", "y_max", "band_nodes"):
+        assert got[k] == want[k], k
+    assert got["theta"] == pytest.approx(want["theta"], rel=1e-14)
+    assert 30.0 < got["theta"] < 90.0   # the droplet's solid parameter -0.2 wets the shelf
+
+
+def test_contact_angle_errors(sclbm):
+    nx, ny = 32, 24
+    d = sclbm.Domain(nx, ny, np.ones(nx * ny, np.int32),
+                     sclbm.make_params(ncomp=2, rho_ref=(1.0, 1.0)), sclbm.FP64)
+    from sc_lbm_b200 import workloads as W
+    d.upload_f(0, W.populations(np.full(nx * ny, 2.0)))
+    d.upload_f(1, W.populations(np.full(nx * ny, 0.06)))
+    with pytest.raises(IndexError):
+        d.contact_angle(0)          # no droplet: empty band
+    rb = np.full((ny, nx), 2.0)
+    rd = np.full((ny, nx), 0.06)
+    rb[12, 5:20], rd[12, 5:20] = 0.7, 1.3   # a band of one row
+    d.upload_f(0, W.populations(rb.ravel()))
+    d.upload_f(1, W.populations(rd.ravel()))
+    with pytest.raises(IndexError):
+        d.contact_angle(0)
+    with pytest.raises(ValueError):
+        d.contact_angle(2)

@@ -269,8 +269,11 @@ int sclbm_domain_mass_momentum(sclbm_domain *d, double out[7]);
  *       its fluid nodes only (populations staged in shared memory), for
  *       lattices with solid nodes (all-fluid lattices run variant 2);
  *   7 = variant 2 with 64-bit element offsets (what lattices of 2^32/9 nodes
- *       and more always run; the other variants use 32-bit offsets).
- * tile_y = rows per tile of variants 1, 2 and 4-7 (0 keeps the default). */
+ *       and more always run; the other variants use 32-bit offsets);
+ *   8 = variant 2 with solid lanes running the collision beside the fluid
+ *       ones and storing zeros into their own slots (no branch around the
+ *       collision; every slot written each step).
+ * tile_y = rows per tile of variants 1, 2 and 4-8 (0 keeps the default). */
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y);
 /* Threads per tile of the register-tile kernel (variants 1, 2): 64 or 128. */
 int sclbm_domain_set_threads(sclbm_domain *d, int tx);
@@ -379,7 +382,8 @@ void sclbm_batch_destroy(sclbm_batch *b);
  * list, tile_y rows per tile, register-tile body; 3 = 128-column strips x
  * row bands of one common height, pipelined body (FP64 and FP32 storage);
  * 5 = tile list with the load-ahead body, 6 = tile list with the compacted
- * fluid-lane body (FP32 and FP16 storage). */
+ * fluid-lane body, 8 = tile list with the uniform solid body (domain variant
+ * 8) (5, 6 and 8: FP32 and FP16 storage). */
 int sclbm_batch_set_kernel(sclbm_batch *b, int variant);
 /* advance every domain nsteps; use_graph = 1 replays a captured CUDA graph */
 int sclbm_batch_step(sclbm_batch *b, int nsteps, int use_graph);

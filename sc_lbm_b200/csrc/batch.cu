@@ -36,8 +36,8 @@ struct sclbm_batch {
     int ntiles = 0, grid = 0, parity = 0;
     int use_units = 1;
     int auto_units = 1; // tuned choice for variant 0
-    int body = BODY_TILE;          // tile-list body: 2 register tile, 5 load ahead, 6 compacted
-    int grid_body[3] = {0, 0, 0};  // resident grid of each body
+    int body = BODY_TILE; // tile-list body: 2 register tile, 5 load ahead, 6 compacted, 8 uniform
+    int grid_body[BODY_COUNT] = {};  // resident grid of each body
     int flags = 0;                 // KF_FORCE / KF_SOLID if any domain needs them
     cudaGraphExec_t graph[2] = {nullptr, nullptr}; // by starting parity
     cudaStream_t graph_stream = nullptr;
@@ -157,7 +157,7 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
     int per_sm = batch_blocks_per_sm(b->prec);
     if (per_sm < 1) per_sm = 1;
     b->grid = std::max(1, std::min(b->ntiles, per_sm * sm_count()));
-    for (int body = 0; body < 3; ++body) {
+    for (int body = 0; body < BODY_COUNT; ++body) {
         const int pb = b->prec == SCLBM_FP64 ? per_sm : std::max(1, batch_blocks_per_sm(b->prec, body));
         b->grid_body[body] = std::max(1, std::min(b->ntiles, pb * sm_count()));
     }
@@ -218,15 +218,18 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
 int sclbm_batch_set_kernel(sclbm_batch *b, int variant)
 {
     if (!b) return set_error(SCLBM_E_INVALID_ARGUMENT, "null batch");
-    if (variant != 0 && variant != 2 && variant != 3 && variant != 5 && variant != 6)
-        return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0, 2, 3, 5 or 6");
+    if (variant != 0 && variant != 2 && variant != 3 && variant != 5 && variant != 6 && variant != 8)
+        return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0, 2, 3, 5, 6 or 8");
     if (variant == 3 && b->prec == SCLBM_FP16_SHIFTED)
         return set_error(SCLBM_E_INVALID_ARGUMENT, "the FP16 form uses the tile list (variant 2)");
-    if ((variant == 5 || variant == 6) && b->prec == SCLBM_FP64)
+    if ((variant == 5 || variant == 6 || variant == 8) && b->prec == SCLBM_FP64)
         return set_error(SCLBM_E_INVALID_ARGUMENT,
-                         "the load-ahead and compacted tile lists are for FP32/FP16 storage");
+                         "the load-ahead, compacted and uniform tile lists are for FP32/FP16 storage");
     b->use_units = variant == 3 || (variant == 0 && b->auto_units);
-    b->body = variant == 5 ? BODY_AHEAD : (variant == 6 ? BODY_COMPACT : BODY_TILE);
+    b->body = variant == 5   ? BODY_AHEAD
+              : variant == 6 ? BODY_COMPACT
+              : variant == 8 ? BODY_UNIFORM
+                             : BODY_TILE;
     for (auto &g : b->graph)
         if (g) {
             cudaGraphExecDestroy(g);

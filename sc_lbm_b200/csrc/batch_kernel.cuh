@@ -57,15 +57,15 @@ __global__ void __launch_bounds__(BATCH_TX, (sizeof(T) == 8 ? 1 : 5))
 
 // flags: KF_FORCE / KF_SOLID when any domain of the batch has a volume force /
 // a solid node (the body drops what no domain needs)
-template <typename S, typename T, bool AHEAD = false, bool COMPACT = false>
+template <typename S, typename T, bool AHEAD = false, bool COMPACT = false, int UNI = 0>
 inline cudaError_t launch_batch_t(const Fused2Args<S, T> *doms, const TileRef *tiles, int ntiles,
                                   int parity, int grid, int flags, cudaStream_t s)
 {
     // batches with solid nodes run the force + solid body (the force vector is
     // zero where no force is set); it compiled leaner than the solid-only one
     if (AHEAD || (flags & KF_SOLID))
-        k_batch2<S, T, KF_FORCE | KF_SOLID, AHEAD, COMPACT><<<grid, BATCH_TX, 0, s>>>(doms, tiles,
-                                                                                  ntiles, parity);
+        k_batch2<S, T, KF_FORCE | KF_SOLID | UNI, AHEAD, COMPACT><<<grid, BATCH_TX, 0, s>>>(
+            doms, tiles, ntiles, parity);
     else if (flags == KF_FORCE)
         k_batch2<S, T, KF_FORCE><<<grid, BATCH_TX, 0, s>>>(doms, tiles, ntiles, parity);
     else
@@ -73,18 +73,19 @@ inline cudaError_t launch_batch_t(const Fused2Args<S, T> *doms, const TileRef *t
     return cudaGetLastError();
 }
 
-template <typename S, typename T, bool AHEAD = false, bool COMPACT = false>
+template <typename S, typename T, bool AHEAD = false, bool COMPACT = false, int UNI = 0>
 inline int batch_blocks_per_sm_t()
 {
     int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &n, k_batch2<S, T, KF_FORCE | KF_SOLID, AHEAD, COMPACT>, BATCH_TX, 0) != cudaSuccess)
+            &n, k_batch2<S, T, KF_FORCE | KF_SOLID | UNI, AHEAD, COMPACT>, BATCH_TX, 0) !=
+        cudaSuccess)
         return 1;
     return n;
 }
 
 // tile body of the FP32-arithmetic batches (ignored for FP64)
-enum BatchBody { BODY_TILE = 0, BODY_AHEAD = 1, BODY_COMPACT = 2 };
+enum BatchBody { BODY_TILE = 0, BODY_AHEAD = 1, BODY_COMPACT = 2, BODY_UNIFORM = 3, BODY_COUNT = 4 };
 cudaError_t launch_batch_fp64(const Fused2Args<double, double> *doms, const TileRef *tiles,
                               int ntiles, int parity, int grid, int flags, cudaStream_t s);
 cudaError_t launch_batch_f32(const Fused2Args<float, float> *doms, const TileRef *tiles,

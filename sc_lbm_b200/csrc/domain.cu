@@ -327,8 +327,9 @@ static cudaError_t step_one(const sclbm_domain *d, cudaStream_t s)
         if constexpr (sizeof(S) == 8) return launch_fused2_async_fp64(a, s);
         else if constexpr (sizeof(S) == 4) return launch_fused2_async_f32(a, s);
     }
-    // variant 1: two pass; 4: register tile with L2 row prefetch; variant 2
-    // (and the FP16 form): register-tile single pass
+    // variant 1: two pass; 4: register tile with L2 row prefetch; 8: register
+    // tile with the uniform solid form; variant 2 (and the FP16 form):
+    // register-tile single pass
     const int v = d->variant == 1 || d->variant >= 4 ? d->variant : 0;
     if constexpr (sizeof(S) == 8) return launch_fused2_fp64(a, v, d->tx, s);
     else if constexpr (sizeof(S) == 4) return launch_fused2_f32(a, v, d->tx, s);
@@ -439,7 +440,7 @@ fail:
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y)
 {
     if (!d) return set_error(SCLBM_E_INVALID_ARGUMENT, "null domain");
-    if (variant < 0 || variant > 7) return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0..7");
+    if (variant < 0 || variant > 8) return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0..8");
     if (tile_y < 0 || tile_y > 4096) return set_error(SCLBM_E_INVALID_ARGUMENT, "bad tile_y");
     if (variant == 1 && !d->rho_tmp[0] && d->ncomp == 2) {
         const size_t es = d->prec == SCLBM_FP64 ? 8 : 4;

@@ -44,6 +44,10 @@ namespace sclbm {
 // specialisation flags of the fused kernels
 constexpr int KF_FORCE = 1; // a volume force is added to at least one component
 constexpr int KF_SOLID = 2; // the lattice has solid nodes
+// with KF_SOLID: solid lanes run the collision alongside the fluid ones (no
+// branch around it) and store zeros into their own slots, so every lane of a
+// warp issues the same instructions and every slot is written each step
+constexpr int KF_UNIFORM = 4;
 
 template <typename S> struct Store;
 template <> struct Store<double> {
@@ -157,13 +161,16 @@ inline bool needs_wide_offsets(size_t N) { return 9 * (unsigned long long)N >= (
 
 template <typename S, typename T, bool SOLID, bool WIDE = false>
 __device__ __forceinline__ void push_one(const Fused2Args<S, T> &a, const int k, const int i,
-                                         const T v, const bool nf, const Nbr &n)
+                                         const T v, const uint32_t nf, const Nbr &n)
 {
     if (i == 0 || !SOLID) {
         Store<S>::st(a.fout[k] + elem<WIDE>(i, a.N, n.nb[i]), v);
     } else {
-        const Off<WIDE> off = nf ? elem<WIDE>(i, a.N, n.nb[i]) : elem<WIDE>(opp(i), a.N, n.nb[0]);
-        Store<S>::st(a.fout[k] + off, v);
+        // nf is 0 or 1: the destination is masked in, which leaves the
+        // compiler no select to turn into a divergent branch
+        using O = Off<WIDE>;
+        const O to = elem<WIDE>(i, a.N, n.nb[i]), back = elem<WIDE>(opp(i), a.N, n.nb[0]);
+        Store<S>::st(a.fout[k] + (back ^ ((to ^ back) & (O(0) - O(nf)))), v);
     }
 }
 
@@ -178,8 +185,12 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
 {
     constexpr bool EXACT = sizeof(T) == 8;
     constexpr bool FORCE = (FLAGS & KF_FORCE) != 0, SOLID = (FLAGS & KF_SOLID) != 0;
+    constexpr bool UNIFORM = SOLID && (FLAGS & KF_UNIFORM) != 0;
     const uint32_t node = n.nb[0];
-    if (SOLID && !st.m[1][st.c]) {
+    // a solid lane of the uniform form treats every neighbour as solid: its
+    // nine stores then land in its own slots, and carry zeros
+    const bool self_fluid = !SOLID || st.m[1][st.c] != 0;
+    if (SOLID && !UNIFORM && !self_fluid) {
         // solid node: the reference's stream leaves zeros (src/lbm.cpp:431-434);
         // on the domain path both buffers already hold them
         if (!a.solids_zero) {
@@ -190,18 +201,20 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
         }
         return;
     }
-    bool nf[9];
+    // nf[i] = 1 when the neighbour along c_i is a fluid node (mask bytes are 0 or 1)
+    uint32_t nf[9];
     T p0[9], p1[9];
+    const uint32_t self_u = SOLID ? (uint32_t)st.m[1][st.c] : 1u;
 #pragma unroll
     for (int i = 1; i < 9; ++i) {
         const int sl = cy(i) + 1;
         const int col = st.c + cx(i);
-        nf[i] = SOLID ? st.m[sl][col] != 0 : true;
+        nf[i] = SOLID ? (uint32_t)st.m[sl][col] & (UNIFORM ? self_u : 1u) : 1u;
         const V2<T> v = st.r[sl][col];
         p0[i] = v.x;
         p1[i] = v.y;
     }
-    nf[0] = true;
+    nf[0] = 1u;
     const V2<T> self = st.r[1][st.c];
     const T psi0 = self.x, psi1 = self.y;
     if constexpr (EXACT) {
@@ -211,7 +224,7 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
 #pragma unroll
         for (int i = 1; i < 9; ++i) {
             const double wcx = w_sc(i) * cx(i), wcy = w_sc(i) * cy(i);
-            const bool f = nf[i];
+            const bool f = nf[i] != 0u;
             F0x = f ? F0x + wcx * p1[i] : F0x;
             F0y = f ? F0y + wcy * p1[i] : F0y;
             F1x = f ? F1x + wcx * p0[i] : F1x;
@@ -265,6 +278,7 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
                 if constexpr (FORCE) {
                     if (a.c[k].force_on) v += a.c[k].force[i];
                 }
+                if constexpr (UNIFORM) v = self_fluid ? v : 0.0;
                 push_one<S, T, SOLID, WIDE>(a, k, i, v, nf[i], n);
             }
         }
@@ -332,6 +346,7 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
                 float v = fmaf(om, fe - fi, fi);
                 // the force vector is zero for a component without a volume force
                 if constexpr (FORCE) v += a.c[k].force[i];
+                if constexpr (UNIFORM) v = self_fluid ? v : 0.f;
                 push_one<S, T, SOLID, WIDE>(a, k, i, v, nf[i], n);
             }
         }
@@ -706,15 +721,16 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
 
 // resident 128-thread CTAs per SM the register cap aims at: FP32 arithmetic
 // fits 80 registers (six CTAs) with two row buffers and 102 (five) with the
-// third buffer of the load-ahead form; FP64 is left uncapped
-template <typename T, bool AHEAD> constexpr int fused_min_ctas()
+// third buffer of the load-ahead form or the uniform solid form; FP64 is left
+// uncapped
+template <typename T, bool AHEAD, int FLAGS = 0> constexpr int fused_min_ctas()
 {
-    return sizeof(T) == 8 ? 1 : (AHEAD ? 5 : 6);
+    return sizeof(T) == 8 ? 1 : (AHEAD || (FLAGS & KF_UNIFORM) ? 5 : 6);
 }
 
 template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS, bool PF = false,
           bool AHEAD = false, bool COMPACT = false, bool WIDE = false>
-__global__ void __launch_bounds__(TX, (fused_min_ctas<T, AHEAD>()))
+__global__ void __launch_bounds__(TX, (fused_min_ctas<T, AHEAD, FLAGS>()))
     k_fused2(const __grid_constant__ Fused2Args<S, T> a)
 {
     __shared__ V2<T> s_rho[4][TX];
@@ -845,22 +861,25 @@ inline cudaError_t launch_fused2_f(const Fused2Args<S, T> &a, cudaStream_t s)
     return cudaGetLastError();
 }
 
-template <typename S, typename T, int TX, bool PF = false, bool AHEAD = false, bool COMPACT = false>
+template <typename S, typename T, int TX, bool PF = false, bool AHEAD = false, bool COMPACT = false,
+          int UNI = 0>
 inline cudaError_t launch_fused2_tx(const Fused2Args<S, T> &a, bool two_pass, cudaStream_t s)
 {
     if (two_pass) return launch_fused2_f<S, T, TX, true, KF_FORCE | KF_SOLID>(a, s);
     switch (kernel_flags(a)) {
     case 0: return launch_fused2_f<S, T, TX, false, 0, PF, AHEAD>(a, s);
     case KF_FORCE: return launch_fused2_f<S, T, TX, false, KF_FORCE, PF, AHEAD>(a, s);
-    case KF_SOLID: return launch_fused2_f<S, T, TX, false, KF_SOLID, PF, AHEAD, COMPACT>(a, s);
-    default: return launch_fused2_f<S, T, TX, false, KF_FORCE | KF_SOLID, PF, AHEAD, COMPACT>(a, s);
+    case KF_SOLID: return launch_fused2_f<S, T, TX, false, KF_SOLID | UNI, PF, AHEAD, COMPACT>(a, s);
+    default:
+        return launch_fused2_f<S, T, TX, false, KF_FORCE | KF_SOLID | UNI, PF, AHEAD, COMPACT>(a, s);
     }
 }
 
 // variant 1: two pass; 4: single pass with L2 row prefetch (128 threads);
 // 5: single pass with loads one row ahead (128 threads); 6: single pass with
 // the collision on compacted fluid lanes (lattices with solid nodes; 128
-// threads); otherwise the single-pass register tile
+// threads); 8: the register tile with the uniform solid form (KF_UNIFORM);
+// otherwise the single-pass register tile
 template <typename S, typename T>
 inline cudaError_t launch_fused2_any(const Fused2Args<S, T> &a, int variant, int tx,
                                      cudaStream_t s)
@@ -874,6 +893,7 @@ inline cudaError_t launch_fused2_any(const Fused2Args<S, T> &a, int variant, int
     if (tx == 64) return launch_fused2_tx<S, T, 64>(a, two, s);
     if (variant == 4) return launch_fused2_tx<S, T, 128, true>(a, false, s);
     if (variant == 5) return launch_fused2_tx<S, T, 128, false, true>(a, false, s);
+    if (variant == 8) return launch_fused2_tx<S, T, 128, false, false, false, KF_UNIFORM>(a, false, s);
     if (variant == 6) {
         // FP64's three population rows would exceed the static shared memory
         if constexpr (sizeof(T) == 4) return launch_fused2_tx<S, T, 128, false, false, true>(a, false, s);

@@ -50,6 +50,9 @@ cudaError_t launch_batch_f32(const Fused2Args<float, float> *doms, const TileRef
         return launch_batch_t<float, float, true>(doms, tiles, ntiles, parity, grid, flags, s);
     if (body == BODY_COMPACT)
         return launch_batch_t<float, float, false, true>(doms, tiles, ntiles, parity, grid, flags, s);
+    if (body == BODY_UNIFORM)
+        return launch_batch_t<float, float, false, false, KF_UNIFORM>(doms, tiles, ntiles, parity, grid,
+                                                                 flags, s);
     return launch_batch_t<float, float>(doms, tiles, ntiles, parity, grid, flags, s);
 }
 cudaError_t launch_batch_f16(const Fused2Args<__half, float> *doms, const TileRef *tiles,
@@ -59,6 +62,9 @@ cudaError_t launch_batch_f16(const Fused2Args<__half, float> *doms, const TileRe
         return launch_batch_t<__half, float, true>(doms, tiles, ntiles, parity, grid, flags, s);
     if (body == BODY_COMPACT)
         return launch_batch_t<__half, float, false, true>(doms, tiles, ntiles, parity, grid, flags, s);
+    if (body == BODY_UNIFORM)
+        return launch_batch_t<__half, float, false, false, KF_UNIFORM>(doms, tiles, ntiles, parity, grid,
+                                                                 flags, s);
     return launch_batch_t<__half, float>(doms, tiles, ntiles, parity, grid, flags, s);
 }
 int batch_blocks_per_sm_fp64();
@@ -69,10 +75,12 @@ int batch_blocks_per_sm(sclbm_precision p, int body)
     case SCLBM_FP32_SHIFTED:
         return body == BODY_AHEAD     ? batch_blocks_per_sm_t<float, float, true>()
                : body == BODY_COMPACT ? batch_blocks_per_sm_t<float, float, false, true>()
+               : body == BODY_UNIFORM ? batch_blocks_per_sm_t<float, float, false, false, KF_UNIFORM>()
                                       : batch_blocks_per_sm_t<float, float>();
     default:
         return body == BODY_AHEAD     ? batch_blocks_per_sm_t<__half, float, true>()
                : body == BODY_COMPACT ? batch_blocks_per_sm_t<__half, float, false, true>()
+               : body == BODY_UNIFORM ? batch_blocks_per_sm_t<__half, float, false, false, KF_UNIFORM>()
                                       : batch_blocks_per_sm_t<__half, float>();
     }
 }

@@ -71,7 +71,7 @@ def test_domain_fp64_bit_exact(sclbm, name):
 @pytest.mark.parametrize("tx,tile_y,variant", [(64, 3, 2), (128, 8, 2), (128, 1, 2), (128, 5, 1),
                                                (64, 64, 1), (128, 0, 0), (128, 0, 3), (128, 0, 4),
                                                (128, 3, 4), (128, 0, 5), (128, 4, 5),
-                                               (128, 0, 7)])
+                                               (128, 0, 7), (128, 0, 8), (128, 3, 8)])
 def test_domain_fp64_tiling_invariant(sclbm, tx, tile_y, variant):
     """Kernel variant (pipelined persistent, two pass, register tile, register
     tile with L2 prefetch) and tile shape do not change a single bit."""
@@ -147,7 +147,7 @@ def test_shifted_forms_density_error(sclbm, oracle, name, steps, prec, tol_max, 
 
 @pytest.mark.parametrize("variant,tile_y", [(1, 4), (4, 0), (4, 7), (3, 0), (5, 0), (5, 7),
                                             (5, 1), (5, 2), (6, 0), (6, 1), (6, 5), (6, 64),
-                                            (7, 0), (7, 3)])
+                                            (7, 0), (7, 3), (8, 0), (8, 5)])
 def test_shifted_variants_match_register_tile(sclbm, variant, tile_y):
     """The shifted forms give the same bytes with every kernel variant."""
     for prec in (sclbm.FP32_SHIFTED, sclbm.FP16_SHIFTED):
@@ -206,7 +206,8 @@ def test_batch_matches_individual_domains(sclbm):
                                 (sclbm.FP32_SHIFTED, False, 3), (sclbm.FP64, False, 2),
                                 (sclbm.FP16_SHIFTED, False, 0), (sclbm.FP32_SHIFTED, True, 5),
                                 (sclbm.FP16_SHIFTED, False, 5), (sclbm.FP32_SHIFTED, True, 6),
-                                (sclbm.FP16_SHIFTED, False, 6)):
+                                (sclbm.FP16_SHIFTED, False, 6), (sclbm.FP32_SHIFTED, True, 8),
+                                (sclbm.FP16_SHIFTED, True, 8)):
         rr = (0.8, 1.2)
         solo = [gpu_runner.run_domain(sclbm, dict(RUNS[n], steps=45), prec, rho_ref=rr) for n in names]
         doms = [gpu_runner.make_domain(sclbm, RUNS[n], prec, rho_ref=rr) for n in names]

@@ -272,7 +272,9 @@ int sclbm_domain_mass_momentum(sclbm_domain *d, double out[7]);
  *       and more always run; the other variants use 32-bit offsets);
  *   8 = variant 2 with solid lanes running the collision beside the fluid
  *       ones and storing zeros into their own slots (no branch around the
- *       collision; every slot written each step).
+ *       collision; every slot written each step);
+ *   9 = variant 3 with the solid form of variant 8 (FP64 and FP32 storage;
+ *       FP16 runs variant 2).
  * tile_y = rows per tile of variants 1, 2 and 4-8 (0 keeps the default). */
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y);
 /* Threads per tile of the register-tile kernel (variants 1, 2): 64 or 128. */

@@ -322,10 +322,12 @@ static cudaError_t step_one(const sclbm_domain *d, cudaStream_t s)
     // except for FP64 storage on a lattice with solid nodes, where the pipelined
     // kernel is faster (4096^2: 16.98 vs 16.55 GLUPS all-fluid; 13.6 vs 11.4 at
     // 60 % fluid); 3 forces the pipelined kernel
-    const bool pipelined = d->variant == 3 || (d->variant == 0 && sizeof(S) == 8 && d->has_solid);
+    const bool pipelined = d->variant == 3 || d->variant == 9 ||
+                           (d->variant == 0 && sizeof(S) == 8 && d->has_solid);
     if (pipelined) {
-        if constexpr (sizeof(S) == 8) return launch_fused2_async_fp64(a, s);
-        else if constexpr (sizeof(S) == 4) return launch_fused2_async_f32(a, s);
+        const bool uni = d->variant == 9;
+        if constexpr (sizeof(S) == 8) return launch_fused2_async_fp64(a, s, uni);
+        else if constexpr (sizeof(S) == 4) return launch_fused2_async_f32(a, s, uni);
     }
     // variant 1: two pass; 4: register tile with L2 row prefetch; 8: register
     // tile with the uniform solid form; variant 2 (and the FP16 form):
@@ -440,7 +442,7 @@ fail:
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y)
 {
     if (!d) return set_error(SCLBM_E_INVALID_ARGUMENT, "null domain");
-    if (variant < 0 || variant > 8) return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0..8");
+    if (variant < 0 || variant > 9) return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0..9");
     if (tile_y < 0 || tile_y > 4096) return set_error(SCLBM_E_INVALID_ARGUMENT, "bad tile_y");
     if (variant == 1 && !d->rho_tmp[0] && d->ncomp == 2) {
         const size_t es = d->prec == SCLBM_FP64 ? 8 : 4;

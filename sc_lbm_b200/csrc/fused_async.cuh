@@ -212,14 +212,15 @@ inline cudaError_t launch_fused2_async_f(const Fused2Args<S, T> &a, cudaStream_t
     return cudaGetLastError();
 }
 
-template <typename S, typename T, int TX, int R>
+// UNI = KF_UNIFORM: lattices with solid nodes run the uniform solid form
+template <typename S, typename T, int TX, int R, int UNI = 0>
 inline cudaError_t launch_fused2_async_t(const Fused2Args<S, T> &a, cudaStream_t s)
 {
     switch (kernel_flags(a)) {
     case 0: return launch_fused2_async_f<S, T, TX, R, 0>(a, s);
     case KF_FORCE: return launch_fused2_async_f<S, T, TX, R, KF_FORCE>(a, s);
-    case KF_SOLID: return launch_fused2_async_f<S, T, TX, R, KF_SOLID>(a, s);
-    default: return launch_fused2_async_f<S, T, TX, R, KF_FORCE | KF_SOLID>(a, s);
+    case KF_SOLID: return launch_fused2_async_f<S, T, TX, R, KF_SOLID | UNI>(a, s);
+    default: return launch_fused2_async_f<S, T, TX, R, KF_FORCE | KF_SOLID | UNI>(a, s);
     }
 }
 

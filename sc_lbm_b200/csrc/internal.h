@@ -119,8 +119,11 @@ cudaError_t launch_fused1_f16(const Fused1Args<__half, float> &a, cudaStream_t s
 // pipelined single-pass kernels (fused_async.cuh): 128-column strips cut into
 // row bands; the batched form walks a list of (domain, strip, band) tiles
 struct BandTile;
-cudaError_t launch_fused2_async_fp64(const Fused2Args<double, double> &a, cudaStream_t s);
-cudaError_t launch_fused2_async_f32(const Fused2Args<float, float> &a, cudaStream_t s);
+// uniform: lattices with solid nodes run the uniform solid form (KF_UNIFORM)
+cudaError_t launch_fused2_async_fp64(const Fused2Args<double, double> &a, cudaStream_t s,
+                                     bool uniform = false);
+cudaError_t launch_fused2_async_f32(const Fused2Args<float, float> &a, cudaStream_t s,
+                                    bool uniform = false);
 cudaError_t launch_batch2_async_fp64(const Fused2Args<double, double> *doms, const BandTile *tiles,
                                      int ntiles, int grid, int parity, cudaStream_t s);
 cudaError_t launch_batch2_async_f32(const Fused2Args<float, float> *doms, const BandTile *tiles,

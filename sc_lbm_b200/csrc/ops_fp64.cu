@@ -419,8 +419,10 @@ int batch_blocks_per_sm_fp64() { return batch_blocks_per_sm_t<double, double>();
 // pipelined persistent FP64 kernels (-fmad=false keeps them bit-exact)
 #include "fused_async.cuh"
 namespace sclbm {
-cudaError_t launch_fused2_async_fp64(const Fused2Args<double, double> &a, cudaStream_t s)
+cudaError_t launch_fused2_async_fp64(const Fused2Args<double, double> &a, cudaStream_t s,
+                                     bool uniform)
 {
+    if (uniform) return launch_fused2_async_t<double, double, 128, 3, KF_UNIFORM>(a, s);
     return launch_fused2_async_t<double, double, 128, 3>(a, s);
 }
 cudaError_t launch_batch2_async_fp64(const Fused2Args<double, double> *doms, const BandTile *tiles,

@@ -88,8 +88,9 @@ int batch_blocks_per_sm(sclbm_precision p, int body)
 
 #include "fused_async.cuh"
 namespace sclbm {
-cudaError_t launch_fused2_async_f32(const Fused2Args<float, float> &a, cudaStream_t s)
+cudaError_t launch_fused2_async_f32(const Fused2Args<float, float> &a, cudaStream_t s, bool uniform)
 {
+    if (uniform) return launch_fused2_async_t<float, float, 128, 4, KF_UNIFORM>(a, s);
     return launch_fused2_async_t<float, float, 128, 4>(a, s);
 }
 cudaError_t launch_batch2_async_f32(const Fused2Args<float, float> *doms, const BandTile *tiles,

@@ -71,7 +71,8 @@ def test_domain_fp64_bit_exact(sclbm, name):
 @pytest.mark.parametrize("tx,tile_y,variant", [(64, 3, 2), (128, 8, 2), (128, 1, 2), (128, 5, 1),
                                                (64, 64, 1), (128, 0, 0), (128, 0, 3), (128, 0, 4),
                                                (128, 3, 4), (128, 0, 5), (128, 4, 5),
-                                               (128, 0, 7), (128, 0, 8), (128, 3, 8)])
+                                               (128, 0, 7), (128, 0, 8), (128, 3, 8),
+                                               (128, 0, 9)])
 def test_domain_fp64_tiling_invariant(sclbm, tx, tile_y, variant):
     """Kernel variant (pipelined persistent, two pass, register tile, register
     tile with L2 prefetch) and tile shape do not change a single bit."""
@@ -147,7 +148,7 @@ def test_shifted_forms_density_error(sclbm, oracle, name, steps, prec, tol_max, 
 
 @pytest.mark.parametrize("variant,tile_y", [(1, 4), (4, 0), (4, 7), (3, 0), (5, 0), (5, 7),
                                             (5, 1), (5, 2), (6, 0), (6, 1), (6, 5), (6, 64),
-                                            (7, 0), (7, 3), (8, 0), (8, 5)])
+                                            (7, 0), (7, 3), (8, 0), (8, 5), (9, 0)])
 def test_shifted_variants_match_register_tile(sclbm, variant, tile_y):
     """The shifted forms give the same bytes with every kernel variant."""
     for prec in (sclbm.FP32_SHIFTED, sclbm.FP16_SHIFTED):

@@ -254,8 +254,9 @@ int sclbm_domain_step(sclbm_domain *d, int nsteps);
  * FP64 (out[3*comp + 0..2]); out[6] = number of non-finite populations. */
 int sclbm_domain_mass_momentum(sclbm_domain *d, double out[7]);
 /* Kernel selection (all variants give identical results):
- *   0 = automatic (default): the fastest measured form -- 3 for FP64
- *       storage on lattices with solid nodes, 2 otherwise;
+ *   0 = automatic (default): the fastest measured form -- on lattices with
+ *       solid nodes 3 for FP64 storage and 8 for FP32/FP16 storage, 2 on
+ *       all-fluid lattices;
  *   1 = two pass (density kernel, then the fused kernel reading it);
  *   2 = single pass, one tile per CTA, population rows held in registers;
  *   3 = single pass, population rows staged through a shared-memory ring by
@@ -385,7 +386,8 @@ void sclbm_batch_destroy(sclbm_batch *b);
  * row bands of one common height, pipelined body (FP64 and FP32 storage);
  * 5 = tile list with the load-ahead body, 6 = tile list with the compacted
  * fluid-lane body, 8 = tile list with the uniform solid body (domain variant
- * 8) (5, 6 and 8: FP32 and FP16 storage). */
+ * 8) (5, 6 and 8: FP32 and FP16 storage).  The automatic tile list of FP32
+ * and FP16 batches holding solid nodes runs the uniform body. */
 int sclbm_batch_set_kernel(sclbm_batch *b, int variant);
 /* advance every domain nsteps; use_graph = 1 replays a captured CUDA graph */
 int sclbm_batch_step(sclbm_batch *b, int nsteps, int use_graph);

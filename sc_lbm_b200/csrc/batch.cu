@@ -37,6 +37,7 @@ struct sclbm_batch {
     int use_units = 1;
     int auto_units = 1; // tuned choice for variant 0
     int body = BODY_TILE; // tile-list body: 2 register tile, 5 load ahead, 6 compacted, 8 uniform
+    int auto_body = BODY_TILE; // tile-list body of variant 0
     int grid_body[BODY_COUNT] = {};  // resident grid of each body
     int flags = 0;                 // KF_FORCE / KF_SOLID if any domain needs them
     cudaGraphExec_t graph[2] = {nullptr, nullptr}; // by starting parity
@@ -171,6 +172,10 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
     // Default: the tuned variant of the size classes holding most nodes (the
     // FP16 form has no band kernel)
     b->auto_units = b->prec != SCLBM_FP16_SHIFTED && nodes_units > nodes_tiles;
+    // FP32/FP16 tile lists with solid nodes: the uniform solid body (512-domain
+    // ensemble, FP32: 21.7 vs 19.6 GLUPS)
+    b->auto_body = (b->flags & KF_SOLID) && b->prec != SCLBM_FP64 ? BODY_UNIFORM : BODY_TILE;
+    b->body = b->auto_body;
     b->use_units = b->auto_units;
     std::vector<BandTile> bands;
     if (b->prec != SCLBM_FP16_SHIFTED) {
@@ -229,6 +234,7 @@ int sclbm_batch_set_kernel(sclbm_batch *b, int variant)
     b->body = variant == 5   ? BODY_AHEAD
               : variant == 6 ? BODY_COMPACT
               : variant == 8 ? BODY_UNIFORM
+              : variant == 0 ? b->auto_body
                              : BODY_TILE;
     for (auto &g : b->graph)
         if (g) {

@@ -369,6 +369,26 @@ int sclbm_domain_profile(sclbm_domain *d, int comp, int axis, double *prof, size
 int sclbm_domain_contact_angle(sclbm_domain *d, int bulk, double rho_bulk, double rho_disp,
                                double out[9]);
 
+/* ------------------------------------------------------------- slab halos
+ * A lattice cut into row slabs (one per GPU, or several on one GPU): a slab
+ * owning global rows [y0, y1) is a domain of y1 - y0 + 2 H rows whose first and
+ * last H rows are ghost copies of the neighbouring slabs' rows (the lattice's
+ * periodic wrap decides the neighbours).  k steps between exchanges need
+ * H >= 2 k; owned rows then stay bit-identical to stepping the whole lattice.
+ * The slab decomposition of tests/lbm/lbm_matlab/two_phase_flow/main_droplet.m
+ * (:162-465) with whole population rows as the halo.  Buffers are device
+ * memory of sclbm_domain_halo_bytes(d, H) bytes, laid out [component][direction]
+ * [H rows][nx] in the storage type; the copies are queued on the library
+ * stream.
+ *   pack side 0: the first H owned rows (for the slab below), side 1: the
+ *   last H owned rows (for the slab above);
+ *   unpack side 0: into the H ghost rows below the owned rows, side 1: into
+ *   the H ghost rows above.
+ * SCLBM_E_OUT_OF_RANGE when H < 1 or 3 H > ny. */
+size_t sclbm_domain_halo_bytes(const sclbm_domain *d, int rows);
+int sclbm_domain_halo_pack(sclbm_domain *d, int rows, int side, void *dst);
+int sclbm_domain_halo_unpack(sclbm_domain *d, int rows, int side, const void *src);
+
 /* ------------------------------------------------------------------- batch
  * Many independent domains of one precision advanced together: one launch
  * per time step walks a tile list drawn from all domains, and the launch

@@ -292,6 +292,16 @@ class Domain(_Handle):
     def set_kernel(self, variant=0, tile_y=0):
         call("sclbm_domain_set_kernel", self._h, int(variant), int(tile_y))
 
+    # halo rows of a slab domain (sc_lbm_b200/slabs.py); ptr = device address
+    def halo_bytes(self, rows) -> int:
+        return int(lib().sclbm_domain_halo_bytes(self._h, int(rows)))
+
+    def halo_pack(self, rows, side, ptr):
+        call("sclbm_domain_halo_pack", self._h, int(rows), int(side), C.c_void_p(int(ptr)))
+
+    def halo_unpack(self, rows, side, ptr):
+        call("sclbm_domain_halo_unpack", self._h, int(rows), int(side), C.c_void_p(int(ptr)))
+
     def set_threads(self, tx):
         call("sclbm_domain_set_threads", self._h, int(tx))
 

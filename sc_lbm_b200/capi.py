@@ -136,6 +136,9 @@ SIGNATURES = {
     "sclbm_domain_velocity_stats": (C.c_int, [_VP, C.c_int, _D]),
     "sclbm_domain_profile": (C.c_int, [_VP, C.c_int, C.c_int, _D, _SZ]),
     "sclbm_domain_contact_angle": (C.c_int, [_VP, C.c_int, C.c_double, C.c_double, _D]),
+    "sclbm_domain_halo_bytes": (_SZ, [_VP, C.c_int]),
+    "sclbm_domain_halo_pack": (C.c_int, [_VP, C.c_int, C.c_int, _VP]),
+    "sclbm_domain_halo_unpack": (C.c_int, [_VP, C.c_int, C.c_int, _VP]),
     "sclbm_geometry_add_random_disks": (C.c_int, [_VP, C.c_double, C.c_int, C.c_int, C.c_uint64,
                                                   C.c_int, C.c_long, C.c_long,
                                                   C.POINTER(_SZ)]),

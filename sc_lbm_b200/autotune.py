@@ -9,8 +9,6 @@ over the candidate shapes of each storage precision:
 
 * tile list (variant 2) with tile_y = 4, 8, 16, 32, 64 rows per tile -- the
   nodes each thread advances per tile (one column per thread, 128 threads);
-  FP32/FP16 storage times the tile body the library runs on porous batches
-  (the uniform solid body, batch kernel 8);
 * strips x bands (variant 3, pipelined body; FP64 and FP32 storage).
 
 It then runs one member of the class in FP64 and in the shifted forms for
@@ -155,8 +153,7 @@ def main():
                 cands = [(2, ty) for ty in TILE_Y] + ([(3, 0)] if pname != "fp16s" else [])
                 res = []
                 for variant, ty in cands:
-                    kern = 8 if variant == 2 and pname != "fp64" else variant
-                    mlups, ms = time_batch(torch, sc, stream, doms, kern, ty or 16,
+                    mlups, ms = time_batch(torch, sc, stream, doms, variant, ty or 16,
                                            args.steps, args.warmup)
                     res.append({"variant": variant, "tile_y": ty or 16, "mlups": round(mlups, 1),
                                 "ms_per_step": round(ms, 5)})

@@ -406,8 +406,10 @@ void sclbm_batch_destroy(sclbm_batch *b);
  * row bands of one common height, pipelined body (FP64 and FP32 storage);
  * 5 = tile list with the load-ahead body, 6 = tile list with the compacted
  * fluid-lane body, 8 = tile list with the uniform solid body (domain variant
- * 8) (5, 6 and 8: FP32 and FP16 storage).  The automatic tile list of FP32
- * and FP16 batches holding solid nodes runs the uniform body. */
+ * 8), 9 = the uniform body on 64-column tiles, two side by side per CTA
+ * (fewer idle lanes on narrow domains) (5, 6, 8 and 9: FP32 and FP16
+ * storage).  The automatic tile list of FP32 and FP16 batches holding solid
+ * nodes runs the uniform body. */
 int sclbm_batch_set_kernel(sclbm_batch *b, int variant);
 /* advance every domain nsteps; use_graph = 1 replays a captured CUDA graph */
 int sclbm_batch_step(sclbm_batch *b, int nsteps, int use_graph);

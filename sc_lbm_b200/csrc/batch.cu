@@ -31,6 +31,8 @@ struct sclbm_batch {
     sclbm_precision prec = SCLBM_FP32_SHIFTED;
     void *d_args = nullptr;  // Fused2Args<S,T>[2*ndom] (parity 0, parity 1)
     TileRef *d_tiles = nullptr;
+    TileRef *d_tiles_half = nullptr; // 64-column tiles of the two-tiles-per-CTA body
+    int ntiles_half = 0;
     BandTile *d_bands = nullptr; // (domain, strip, band) tiles of the pipelined kernel
     int nbands = 0, band_grid = 0, band_rows = 0;
     int ntiles = 0, grid = 0, parity = 0;
@@ -57,11 +59,15 @@ static cudaError_t batch_launch_any(sclbm_batch *b, int parity, cudaStream_t s)
         return launch_batch_fp64((const Fused2Args<double, double> *)b->d_args, b->d_tiles,
                                  b->ntiles, parity, b->grid, b->flags, s);
     case SCLBM_FP32_SHIFTED:
-        return launch_batch_f32((const Fused2Args<float, float> *)b->d_args, b->d_tiles,
-                                b->ntiles, parity, b->grid_body[b->body], b->flags, b->body, s);
+        return launch_batch_f32((const Fused2Args<float, float> *)b->d_args,
+                                b->body == BODY_HALF ? b->d_tiles_half : b->d_tiles,
+                                b->body == BODY_HALF ? b->ntiles_half : b->ntiles, parity,
+                                b->grid_body[b->body], b->flags, b->body, s);
     default:
-        return launch_batch_f16((const Fused2Args<__half, float> *)b->d_args, b->d_tiles,
-                                b->ntiles, parity, b->grid_body[b->body], b->flags, b->body, s);
+        return launch_batch_f16((const Fused2Args<__half, float> *)b->d_args,
+                                b->body == BODY_HALF ? b->d_tiles_half : b->d_tiles,
+                                b->body == BODY_HALF ? b->ntiles_half : b->ntiles, parity,
+                                b->grid_body[b->body], b->flags, b->body, s);
     }
 }
 
@@ -101,6 +107,7 @@ void sclbm_batch_destroy(sclbm_batch *b)
         if (g) cudaGraphExecDestroy(g);
     if (b->d_args) cudaFree(b->d_args);
     if (b->d_tiles) cudaFree(b->d_tiles);
+    if (b->d_tiles_half) cudaFree(b->d_tiles_half);
     if (b->d_bands) cudaFree(b->d_bands);
     delete b;
 }
@@ -121,10 +128,7 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
     b->prec = b->doms[0]->prec;
     b->parity = b->doms[0]->parity;
     std::vector<int> ty(ndomains);
-    std::vector<TileRef> tiles;
-    std::vector<long> cost;
     double nodes_units = 0.0, nodes_tiles = 0.0;
-    const int W = BATCH_TX - 2;
     for (int k = 0; k < ndomains; ++k) {
         sclbm_domain *d = b->doms[k];
         if (!d || d->ncomp != 2 || d->prec != b->prec || d->parity != b->parity) {
@@ -142,25 +146,39 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
         const SclbmTunedShape ts = tuned_shape(d->nx, d->ny, b->prec);
         ty[k] = tile_y_per_domain && tile_y_per_domain[k] > 0 ? tile_y_per_domain[k] : ts.tile_y;
         (ts.variant == 3 ? nodes_units : nodes_tiles) += (double)d->nx * (double)d->ny;
-        for (int yb = 0; yb < (int)d->ny; yb += ty[k])
-            for (int xb = 0; xb < (int)d->nx; xb += W) {
-                tiles.push_back(TileRef{k, xb, yb, 0});
-                cost.push_back((long)std::min(W, (int)d->nx - xb) * (std::min(ty[k], (int)d->ny - yb) + 2));
-            }
     }
-    // largest tiles first
-    std::vector<int> order(tiles.size());
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return cost[a] > cost[c]; });
-    std::vector<TileRef> sorted(tiles.size());
-    for (size_t i = 0; i < order.size(); ++i) sorted[i] = tiles[order[i]];
+    // tile lists of tiles `width` columns wide, largest tiles first
+    auto tile_list = [&](int width) {
+        const int w = width - 2;
+        std::vector<TileRef> list;
+        std::vector<long> cost;
+        for (int k = 0; k < ndomains; ++k) {
+            const sclbm_domain *d = b->doms[k];
+            for (int yb = 0; yb < (int)d->ny; yb += ty[k])
+                for (int xb = 0; xb < (int)d->nx; xb += w) {
+                    list.push_back(TileRef{k, xb, yb, 0});
+                    cost.push_back((long)std::min(w, (int)d->nx - xb) *
+                                   (std::min(ty[k], (int)d->ny - yb) + 2));
+                }
+        }
+        std::vector<int> order(list.size());
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return cost[a] > cost[c]; });
+        std::vector<TileRef> sorted(list.size());
+        for (size_t i = 0; i < order.size(); ++i) sorted[i] = list[order[i]];
+        return sorted;
+    };
+    const std::vector<TileRef> sorted = tile_list(BATCH_TX);
+    const std::vector<TileRef> halves = tile_list(HALF_TX);
     b->ntiles = (int)sorted.size();
+    b->ntiles_half = (int)halves.size();
     int per_sm = batch_blocks_per_sm(b->prec);
     if (per_sm < 1) per_sm = 1;
     b->grid = std::max(1, std::min(b->ntiles, per_sm * sm_count()));
     for (int body = 0; body < BODY_COUNT; ++body) {
         const int pb = b->prec == SCLBM_FP64 ? per_sm : std::max(1, batch_blocks_per_sm(b->prec, body));
-        b->grid_body[body] = std::max(1, std::min(b->ntiles, pb * sm_count()));
+        const int units = body == BODY_HALF ? (b->ntiles_half + 1) / 2 : b->ntiles;
+        b->grid_body[body] = std::max(1, std::min(units, pb * sm_count()));
     }
     switch (b->prec) {
     case SCLBM_FP64: rc = upload_args<double, double>(b, ty); break;
@@ -212,6 +230,11 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
     if (!rc && cudaMemcpy(b->d_tiles, sorted.data(), sorted.size() * sizeof(TileRef),
                           cudaMemcpyHostToDevice) != cudaSuccess)
         rc = set_error(SCLBM_E_CUDA, "tile list upload");
+    if (!rc && cudaMalloc(&b->d_tiles_half, halves.size() * sizeof(TileRef)) != cudaSuccess)
+        rc = set_error(SCLBM_E_CUDA, "tile list allocation");
+    if (!rc && cudaMemcpy(b->d_tiles_half, halves.data(), halves.size() * sizeof(TileRef),
+                          cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = set_error(SCLBM_E_CUDA, "tile list upload");
     if (rc) {
         sclbm_batch_destroy(b);
         return rc;
@@ -223,17 +246,19 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
 int sclbm_batch_set_kernel(sclbm_batch *b, int variant)
 {
     if (!b) return set_error(SCLBM_E_INVALID_ARGUMENT, "null batch");
-    if (variant != 0 && variant != 2 && variant != 3 && variant != 5 && variant != 6 && variant != 8)
-        return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0, 2, 3, 5, 6 or 8");
+    if (variant != 0 && variant != 2 && variant != 3 && variant != 5 && variant != 6 && variant != 8 &&
+        variant != 9)
+        return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0, 2, 3, 5, 6, 8 or 9");
     if (variant == 3 && b->prec == SCLBM_FP16_SHIFTED)
         return set_error(SCLBM_E_INVALID_ARGUMENT, "the FP16 form uses the tile list (variant 2)");
-    if ((variant == 5 || variant == 6 || variant == 8) && b->prec == SCLBM_FP64)
+    if ((variant == 5 || variant == 6 || variant == 8 || variant == 9) && b->prec == SCLBM_FP64)
         return set_error(SCLBM_E_INVALID_ARGUMENT,
                          "the load-ahead, compacted and uniform tile lists are for FP32/FP16 storage");
     b->use_units = variant == 3 || (variant == 0 && b->auto_units);
     b->body = variant == 5   ? BODY_AHEAD
               : variant == 6 ? BODY_COMPACT
               : variant == 8 ? BODY_UNIFORM
+              : variant == 9 ? BODY_HALF
               : variant == 0 ? b->auto_body
                              : BODY_TILE;
     for (auto &g : b->graph)
@@ -247,7 +272,7 @@ int sclbm_batch_set_kernel(sclbm_batch *b, int variant)
 int sclbm_batch_info(const sclbm_batch *b, int *ntiles, int *grid_ctas)
 {
     if (!b) return set_error(SCLBM_E_INVALID_ARGUMENT, "null batch");
-    if (ntiles) *ntiles = b->ntiles;
+    if (ntiles) *ntiles = !b->use_units && b->body == BODY_HALF ? b->ntiles_half : b->ntiles;
     if (grid_ctas)
         *grid_ctas = b->use_units ? b->band_grid : (b->prec == SCLBM_FP64 ? b->grid : b->grid_body[b->body]);
     return SCLBM_OK;

@@ -55,6 +55,63 @@ __global__ void __launch_bounds__(BATCH_TX, (sizeof(T) == 8 ? 1 : 5))
     }
 }
 
+// Two 64-column tiles side by side in each 128-thread CTA: threads 0-63 run
+// tiles 2c, 2c + 2g, ... and threads 64-127 tiles 2c + 1, 2c + 1 + 2g, ... of
+// the 64-column tile list (g = gridDim.x), each half with its own density
+// ring, argument block and named barrier, so the halves never wait on each
+// other.  Narrow domains leave fewer idle lanes than with 128-column tiles
+// (the ensemble's widths 64..512: 88 % of the lanes busy against 81 %).
+constexpr int HALF_TX = BATCH_TX / 2;
+template <typename S, typename T, int FLAGS>
+__global__ void __launch_bounds__(BATCH_TX, (sizeof(T) == 8 ? 1 : 5))
+    k_batch2_half(const Fused2Args<S, T> *__restrict__ doms, const TileRef *__restrict__ tiles,
+                  int ntiles, int parity)
+{
+    __shared__ V2<T> s_rho[2][4][HALF_TX];
+    __shared__ uint8_t s_m[2][4][HALF_TX];
+    __shared__ __align__(16) Fused2Args<S, T> sa[2];
+    static_assert(sizeof(Fused2Args<S, T>) % 4 == 0, "argument block copied as words");
+    const int half = threadIdx.x / HALF_TX, lt = threadIdx.x % HALF_TX;
+    const int bar = 1 + half;
+    int loaded = -1;
+    for (int i = 2 * blockIdx.x + half; i < ntiles; i += 2 * gridDim.x) {
+        const TileRef tr = tiles[i];
+        const int key = 2 * tr.dom + parity;
+        if (key != loaded) { // uniform over the half
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(doms + key);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(&sa[half]);
+            for (int w = lt; w < (int)(sizeof(Fused2Args<S, T>) / 4); w += HALF_TX) dst[w] = src[w];
+            tile_sync<HALF_TX>(bar);
+            loaded = key;
+        }
+        const bool down = ((tr.yb / sa[half].tile_y) & 1) != 0;
+        fused2_tile<S, T, HALF_TX, false, FLAGS>(sa[half], tr.xb, tr.yb, s_rho[half], s_m[half], down,
+                                                 bar);
+        tile_sync<HALF_TX>(bar); // the half's ring and block are reused by its next tile
+    }
+}
+
+template <typename S, typename T>
+inline cudaError_t launch_batch_half_t(const Fused2Args<S, T> *doms, const TileRef *tiles,
+                                       int ntiles, int parity, int grid, int flags, cudaStream_t s)
+{
+    if (flags & KF_SOLID)
+        k_batch2_half<S, T, KF_FORCE | KF_SOLID | KF_UNIFORM><<<grid, BATCH_TX, 0, s>>>(doms, tiles,
+                                                                                      ntiles, parity);
+    else
+        k_batch2_half<S, T, KF_FORCE><<<grid, BATCH_TX, 0, s>>>(doms, tiles, ntiles, parity);
+    return cudaGetLastError();
+}
+
+template <typename S, typename T> inline int batch_half_blocks_per_sm_t()
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &n, k_batch2_half<S, T, KF_FORCE | KF_SOLID | KF_UNIFORM>, BATCH_TX, 0) != cudaSuccess)
+        return 1;
+    return n;
+}
+
 // flags: KF_FORCE / KF_SOLID when any domain of the batch has a volume force /
 // a solid node (the body drops what no domain needs)
 template <typename S, typename T, bool AHEAD = false, bool COMPACT = false, int UNI = 0>
@@ -85,7 +142,14 @@ inline int batch_blocks_per_sm_t()
 }
 
 // tile body of the FP32-arithmetic batches (ignored for FP64)
-enum BatchBody { BODY_TILE = 0, BODY_AHEAD = 1, BODY_COMPACT = 2, BODY_UNIFORM = 3, BODY_COUNT = 4 };
+enum BatchBody {
+    BODY_TILE = 0,
+    BODY_AHEAD = 1,
+    BODY_COMPACT = 2,
+    BODY_UNIFORM = 3,
+    BODY_HALF = 4, // two 64-column tiles per CTA (k_batch2_half), its own tile list
+    BODY_COUNT = 5
+};
 cudaError_t launch_batch_fp64(const Fused2Args<double, double> *doms, const TileRef *tiles,
                               int ntiles, int parity, int grid, int flags, cudaStream_t s);
 cudaError_t launch_batch_f32(const Fused2Args<float, float> *doms, const TileRef *tiles,

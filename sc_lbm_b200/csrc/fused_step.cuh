@@ -608,11 +608,20 @@ __device__ __forceinline__ void fused2_tile_compact(const Fused2Args<S, T> &a, c
 // ends -- and the second read finds them in L2 instead of going to DRAM.
 // Direction changes only the order of the rows; every node gets the same
 // arithmetic and every destination slot the same single write.
+// Barrier of the threads running one tile: the whole CTA (bar = 0), or the TX
+// threads of one part of a CTA that runs several tiles side by side (named
+// barrier bar = 1, 2, ...; TX a multiple of 32, each warp in one part).
+template <int TX> __device__ __forceinline__ void tile_sync(const int bar)
+{
+    if (bar == 0) __syncthreads();
+    else asm volatile("bar.sync %0, %1;" ::"r"(bar), "n"(TX) : "memory");
+}
+
 template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS, bool PF = false,
           bool AHEAD = false, bool WIDE = false>
 __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int xb, const int yb,
                                             V2<T> (&s_rho)[4][TX], uint8_t (&s_m)[4][TX],
-                                            const bool down = false)
+                                            const bool down = false, const int bar = 0)
 {
     if constexpr (AHEAD && !TWO_PASS) {
         fused2_tile_ahead<S, T, TX, FLAGS>(a, xb, yb, s_rho, s_m);
@@ -620,7 +629,8 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
     }
     constexpr bool SOLID = (FLAGS & KF_SOLID) != 0;
     constexpr int W = TX - 2;
-    const int t = threadIdx.x;
+    static_assert((TX & (TX - 1)) == 0, "TX a power of two");
+    const int t = threadIdx.x & (TX - 1); // column of this thread in its tile
     const int nx = a.nx, ny = a.ny;
     const int ncol = min(W, nx - xb);
     const int nrow = min(a.tile_y, ny - yb);
@@ -693,7 +703,7 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
         }
         s_rho[slot][t] = Vec2<T>::make(rho[0], rho[1]);
         s_m[slot][t] = m;
-        __syncthreads();
+        tile_sync<TX>(bar);
 
         if (q >= 1 && interior) {
             // slots of the rows below (sb), at (sc) and above (sa) the node

@@ -53,6 +53,8 @@ cudaError_t launch_batch_f32(const Fused2Args<float, float> *doms, const TileRef
     if (body == BODY_UNIFORM)
         return launch_batch_t<float, float, false, false, KF_UNIFORM>(doms, tiles, ntiles, parity, grid,
                                                                  flags, s);
+    if (body == BODY_HALF)
+        return launch_batch_half_t<float, float>(doms, tiles, ntiles, parity, grid, flags, s);
     return launch_batch_t<float, float>(doms, tiles, ntiles, parity, grid, flags, s);
 }
 cudaError_t launch_batch_f16(const Fused2Args<__half, float> *doms, const TileRef *tiles,
@@ -65,6 +67,8 @@ cudaError_t launch_batch_f16(const Fused2Args<__half, float> *doms, const TileRe
     if (body == BODY_UNIFORM)
         return launch_batch_t<__half, float, false, false, KF_UNIFORM>(doms, tiles, ntiles, parity, grid,
                                                                  flags, s);
+    if (body == BODY_HALF)
+        return launch_batch_half_t<__half, float>(doms, tiles, ntiles, parity, grid, flags, s);
     return launch_batch_t<__half, float>(doms, tiles, ntiles, parity, grid, flags, s);
 }
 int batch_blocks_per_sm_fp64();
@@ -76,11 +80,13 @@ int batch_blocks_per_sm(sclbm_precision p, int body)
         return body == BODY_AHEAD     ? batch_blocks_per_sm_t<float, float, true>()
                : body == BODY_COMPACT ? batch_blocks_per_sm_t<float, float, false, true>()
                : body == BODY_UNIFORM ? batch_blocks_per_sm_t<float, float, false, false, KF_UNIFORM>()
+               : body == BODY_HALF    ? batch_half_blocks_per_sm_t<float, float>()
                                       : batch_blocks_per_sm_t<float, float>();
     default:
         return body == BODY_AHEAD     ? batch_blocks_per_sm_t<__half, float, true>()
                : body == BODY_COMPACT ? batch_blocks_per_sm_t<__half, float, false, true>()
                : body == BODY_UNIFORM ? batch_blocks_per_sm_t<__half, float, false, false, KF_UNIFORM>()
+               : body == BODY_HALF    ? batch_half_blocks_per_sm_t<__half, float>()
                                       : batch_blocks_per_sm_t<__half, float>();
     }
 }

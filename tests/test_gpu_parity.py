@@ -208,7 +208,8 @@ def test_batch_matches_individual_domains(sclbm):
                                 (sclbm.FP16_SHIFTED, False, 0), (sclbm.FP32_SHIFTED, True, 5),
                                 (sclbm.FP16_SHIFTED, False, 5), (sclbm.FP32_SHIFTED, True, 6),
                                 (sclbm.FP16_SHIFTED, False, 6), (sclbm.FP32_SHIFTED, True, 8),
-                                (sclbm.FP16_SHIFTED, True, 8)):
+                                (sclbm.FP16_SHIFTED, True, 8), (sclbm.FP32_SHIFTED, True, 9),
+                                (sclbm.FP16_SHIFTED, False, 9)):
         rr = (0.8, 1.2)
         solo = [gpu_runner.run_domain(sclbm, dict(RUNS[n], steps=45), prec, rho_ref=rr) for n in names]
         doms = [gpu_runner.make_domain(sclbm, RUNS[n], prec, rho_ref=rr) for n in names]

@@ -62,6 +62,32 @@ __global__ void __launch_bounds__(BATCH_TX, (sizeof(T) == 8 ? 1 : 5))
 // other.  Narrow domains leave fewer idle lanes than with 128-column tiles
 // (the ensemble's widths 64..512: 88 % of the lanes busy against 81 %).
 constexpr int HALF_TX = BATCH_TX / 2;
+// the tile loop of half h (named barrier 1 + h)
+template <typename S, typename T, int FLAGS, int BAR>
+__device__ __forceinline__ void batch_half_loop(const Fused2Args<S, T> *__restrict__ doms,
+                                                const TileRef *__restrict__ tiles, int ntiles,
+                                                int parity, V2<T> (&s_rho)[4][HALF_TX],
+                                                uint8_t (&s_m)[4][HALF_TX], Fused2Args<S, T> &sa)
+{
+    const int lt = threadIdx.x % HALF_TX;
+    int loaded = -1;
+    for (int i = 2 * blockIdx.x + (BAR - 1); i < ntiles; i += 2 * gridDim.x) {
+        const TileRef tr = tiles[i];
+        const int key = 2 * tr.dom + parity;
+        if (key != loaded) { // uniform over the half
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(doms + key);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(&sa);
+            for (int w = lt; w < (int)(sizeof(Fused2Args<S, T>) / 4); w += HALF_TX) dst[w] = src[w];
+            tile_sync<HALF_TX, BAR>();
+            loaded = key;
+        }
+        const bool down = ((tr.yb / sa.tile_y) & 1) != 0;
+        fused2_tile<S, T, HALF_TX, false, FLAGS, false, false, false, BAR>(sa, tr.xb, tr.yb, s_rho, s_m,
+                                                                           down);
+        tile_sync<HALF_TX, BAR>(); // the half's ring and block are reused by its next tile
+    }
+}
+
 template <typename S, typename T, int FLAGS>
 __global__ void __launch_bounds__(BATCH_TX, (sizeof(T) == 8 ? 1 : 5))
     k_batch2_half(const Fused2Args<S, T> *__restrict__ doms, const TileRef *__restrict__ tiles,
@@ -71,24 +97,10 @@ __global__ void __launch_bounds__(BATCH_TX, (sizeof(T) == 8 ? 1 : 5))
     __shared__ uint8_t s_m[2][4][HALF_TX];
     __shared__ __align__(16) Fused2Args<S, T> sa[2];
     static_assert(sizeof(Fused2Args<S, T>) % 4 == 0, "argument block copied as words");
-    const int half = threadIdx.x / HALF_TX, lt = threadIdx.x % HALF_TX;
-    const int bar = 1 + half;
-    int loaded = -1;
-    for (int i = 2 * blockIdx.x + half; i < ntiles; i += 2 * gridDim.x) {
-        const TileRef tr = tiles[i];
-        const int key = 2 * tr.dom + parity;
-        if (key != loaded) { // uniform over the half
-            const uint32_t *src = reinterpret_cast<const uint32_t *>(doms + key);
-            uint32_t *dst = reinterpret_cast<uint32_t *>(&sa[half]);
-            for (int w = lt; w < (int)(sizeof(Fused2Args<S, T>) / 4); w += HALF_TX) dst[w] = src[w];
-            tile_sync<HALF_TX>(bar);
-            loaded = key;
-        }
-        const bool down = ((tr.yb / sa[half].tile_y) & 1) != 0;
-        fused2_tile<S, T, HALF_TX, false, FLAGS>(sa[half], tr.xb, tr.yb, s_rho[half], s_m[half], down,
-                                                 bar);
-        tile_sync<HALF_TX>(bar); // the half's ring and block are reused by its next tile
-    }
+    if (threadIdx.x < HALF_TX)
+        batch_half_loop<S, T, FLAGS, 1>(doms, tiles, ntiles, parity, s_rho[0], s_m[0], sa[0]);
+    else
+        batch_half_loop<S, T, FLAGS, 2>(doms, tiles, ntiles, parity, s_rho[1], s_m[1], sa[1]);
 }
 
 template <typename S, typename T>

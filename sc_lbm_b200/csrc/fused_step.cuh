@@ -608,20 +608,22 @@ __device__ __forceinline__ void fused2_tile_compact(const Fused2Args<S, T> &a, c
 // ends -- and the second read finds them in L2 instead of going to DRAM.
 // Direction changes only the order of the rows; every node gets the same
 // arithmetic and every destination slot the same single write.
-// Barrier of the threads running one tile: the whole CTA (bar = 0), or the TX
+// Barrier of the threads running one tile: the whole CTA (BAR = 0), or the TX
 // threads of one part of a CTA that runs several tiles side by side (named
-// barrier bar = 1, 2, ...; TX a multiple of 32, each warp in one part).
-template <int TX> __device__ __forceinline__ void tile_sync(const int bar)
+// barrier BAR = 1, 2, ...; TX a multiple of 32, each warp in one part).  The
+// barrier number is an immediate: a register operand makes ptxas reserve all
+// sixteen barriers of the CTA, which caps residency at four CTAs per SM.
+template <int TX, int BAR> __device__ __forceinline__ void tile_sync()
 {
-    if (bar == 0) __syncthreads();
-    else asm volatile("bar.sync %0, %1;" ::"r"(bar), "n"(TX) : "memory");
+    if constexpr (BAR == 0) __syncthreads();
+    else asm volatile("bar.sync %0, %1;" ::"n"(BAR), "n"(TX) : "memory");
 }
 
 template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS, bool PF = false,
-          bool AHEAD = false, bool WIDE = false>
+          bool AHEAD = false, bool WIDE = false, int BAR = 0>
 __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int xb, const int yb,
                                             V2<T> (&s_rho)[4][TX], uint8_t (&s_m)[4][TX],
-                                            const bool down = false, const int bar = 0)
+                                            const bool down = false)
 {
     if constexpr (AHEAD && !TWO_PASS) {
         fused2_tile_ahead<S, T, TX, FLAGS>(a, xb, yb, s_rho, s_m);
@@ -703,7 +705,7 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
         }
         s_rho[slot][t] = Vec2<T>::make(rho[0], rho[1]);
         s_m[slot][t] = m;
-        tile_sync<TX>(bar);
+        tile_sync<TX, BAR>();
 
         if (q >= 1 && interior) {
             // slots of the rows below (sb), at (sc) and above (sa) the node

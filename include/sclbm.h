@@ -278,7 +278,8 @@ int sclbm_domain_mass_momentum(sclbm_domain *d, double out[7]);
  *       FP16 runs variant 2).
  * tile_y = rows per tile of variants 1, 2 and 4-8 (0 keeps the default). */
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y);
-/* Threads per tile of the register-tile kernel (variants 1, 2): 64 or 128. */
+/* Threads per tile of the register-tile kernel (variants 1, 2, and 8 with
+ * 32 or 128): 32 (one-warp tiles, no CTA barrier), 64 or 128. */
 int sclbm_domain_set_threads(sclbm_domain *d, int tx);
 /* Device bytes held by the domain. */
 size_t sclbm_domain_device_bytes(const sclbm_domain *d);
@@ -407,8 +408,9 @@ void sclbm_batch_destroy(sclbm_batch *b);
  * 5 = tile list with the load-ahead body, 6 = tile list with the compacted
  * fluid-lane body, 8 = tile list with the uniform solid body (domain variant
  * 8), 9 = the uniform body on 64-column tiles, two side by side per CTA
- * (fewer idle lanes on narrow domains) (5, 6, 8 and 9: FP32 and FP16
- * storage).  The automatic tile list of FP32 and FP16 batches holding solid
+ * (fewer idle lanes on narrow domains), 10 = the uniform body on one-warp
+ * 32-column tiles, each warp walking its own tiles (no CTA barrier) (5, 6, 8,
+ * 9 and 10: FP32 and FP16 storage).  The automatic tile list of FP32 and FP16 batches holding solid
  * nodes runs the uniform body. */
 int sclbm_batch_set_kernel(sclbm_batch *b, int variant);
 /* advance every domain nsteps; use_graph = 1 replays a captured CUDA graph */

@@ -33,6 +33,8 @@ struct sclbm_batch {
     TileRef *d_tiles = nullptr;
     TileRef *d_tiles_half = nullptr; // 64-column tiles of the two-tiles-per-CTA body
     int ntiles_half = 0;
+    TileRef *d_tiles_warp = nullptr; // 32-column tiles of the one-tile-per-warp body
+    int ntiles_warp = 0;
     BandTile *d_bands = nullptr; // (domain, strip, band) tiles of the pipelined kernel
     int nbands = 0, band_grid = 0, band_rows = 0;
     int ntiles = 0, grid = 0, parity = 0;
@@ -45,6 +47,16 @@ struct sclbm_batch {
     cudaGraphExec_t graph[2] = {nullptr, nullptr}; // by starting parity
     cudaStream_t graph_stream = nullptr;
 };
+
+// the tile list of the current body
+static const TileRef *batch_tiles(const sclbm_batch *b)
+{
+    return b->body == BODY_HALF ? b->d_tiles_half : b->body == BODY_WARP ? b->d_tiles_warp : b->d_tiles;
+}
+static int batch_ntiles(const sclbm_batch *b)
+{
+    return b->body == BODY_HALF ? b->ntiles_half : b->body == BODY_WARP ? b->ntiles_warp : b->ntiles;
+}
 
 static cudaError_t batch_launch_any(sclbm_batch *b, int parity, cudaStream_t s)
 {
@@ -59,15 +71,11 @@ static cudaError_t batch_launch_any(sclbm_batch *b, int parity, cudaStream_t s)
         return launch_batch_fp64((const Fused2Args<double, double> *)b->d_args, b->d_tiles,
                                  b->ntiles, parity, b->grid, b->flags, s);
     case SCLBM_FP32_SHIFTED:
-        return launch_batch_f32((const Fused2Args<float, float> *)b->d_args,
-                                b->body == BODY_HALF ? b->d_tiles_half : b->d_tiles,
-                                b->body == BODY_HALF ? b->ntiles_half : b->ntiles, parity,
-                                b->grid_body[b->body], b->flags, b->body, s);
+        return launch_batch_f32((const Fused2Args<float, float> *)b->d_args, batch_tiles(b),
+                                batch_ntiles(b), parity, b->grid_body[b->body], b->flags, b->body, s);
     default:
-        return launch_batch_f16((const Fused2Args<__half, float> *)b->d_args,
-                                b->body == BODY_HALF ? b->d_tiles_half : b->d_tiles,
-                                b->body == BODY_HALF ? b->ntiles_half : b->ntiles, parity,
-                                b->grid_body[b->body], b->flags, b->body, s);
+        return launch_batch_f16((const Fused2Args<__half, float> *)b->d_args, batch_tiles(b),
+                                batch_ntiles(b), parity, b->grid_body[b->body], b->flags, b->body, s);
     }
 }
 
@@ -108,6 +116,7 @@ void sclbm_batch_destroy(sclbm_batch *b)
     if (b->d_args) cudaFree(b->d_args);
     if (b->d_tiles) cudaFree(b->d_tiles);
     if (b->d_tiles_half) cudaFree(b->d_tiles_half);
+    if (b->d_tiles_warp) cudaFree(b->d_tiles_warp);
     if (b->d_bands) cudaFree(b->d_bands);
     delete b;
 }
@@ -170,14 +179,18 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
     };
     const std::vector<TileRef> sorted = tile_list(BATCH_TX);
     const std::vector<TileRef> halves = tile_list(HALF_TX);
+    const std::vector<TileRef> warps = tile_list(WARP_TX);
     b->ntiles = (int)sorted.size();
     b->ntiles_half = (int)halves.size();
+    b->ntiles_warp = (int)warps.size();
     int per_sm = batch_blocks_per_sm(b->prec);
     if (per_sm < 1) per_sm = 1;
     b->grid = std::max(1, std::min(b->ntiles, per_sm * sm_count()));
     for (int body = 0; body < BODY_COUNT; ++body) {
         const int pb = b->prec == SCLBM_FP64 ? per_sm : std::max(1, batch_blocks_per_sm(b->prec, body));
-        const int units = body == BODY_HALF ? (b->ntiles_half + 1) / 2 : b->ntiles;
+        const int units = body == BODY_HALF   ? (b->ntiles_half + 1) / 2
+                          : body == BODY_WARP ? (b->ntiles_warp + BATCH_TX / WARP_TX - 1) / (BATCH_TX / WARP_TX)
+                                              : b->ntiles;
         b->grid_body[body] = std::max(1, std::min(units, pb * sm_count()));
     }
     switch (b->prec) {
@@ -230,6 +243,11 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
     if (!rc && cudaMemcpy(b->d_tiles, sorted.data(), sorted.size() * sizeof(TileRef),
                           cudaMemcpyHostToDevice) != cudaSuccess)
         rc = set_error(SCLBM_E_CUDA, "tile list upload");
+    if (!rc && cudaMalloc(&b->d_tiles_warp, warps.size() * sizeof(TileRef)) != cudaSuccess)
+        rc = set_error(SCLBM_E_CUDA, "tile list allocation");
+    if (!rc && cudaMemcpy(b->d_tiles_warp, warps.data(), warps.size() * sizeof(TileRef),
+                          cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = set_error(SCLBM_E_CUDA, "tile list upload");
     if (!rc && cudaMalloc(&b->d_tiles_half, halves.size() * sizeof(TileRef)) != cudaSuccess)
         rc = set_error(SCLBM_E_CUDA, "tile list allocation");
     if (!rc && cudaMemcpy(b->d_tiles_half, halves.data(), halves.size() * sizeof(TileRef),
@@ -247,11 +265,11 @@ int sclbm_batch_set_kernel(sclbm_batch *b, int variant)
 {
     if (!b) return set_error(SCLBM_E_INVALID_ARGUMENT, "null batch");
     if (variant != 0 && variant != 2 && variant != 3 && variant != 5 && variant != 6 && variant != 8 &&
-        variant != 9)
-        return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0, 2, 3, 5, 6, 8 or 9");
+        variant != 9 && variant != 10)
+        return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0, 2, 3, 5, 6, 8, 9 or 10");
     if (variant == 3 && b->prec == SCLBM_FP16_SHIFTED)
         return set_error(SCLBM_E_INVALID_ARGUMENT, "the FP16 form uses the tile list (variant 2)");
-    if ((variant == 5 || variant == 6 || variant == 8 || variant == 9) && b->prec == SCLBM_FP64)
+    if ((variant == 5 || variant == 6 || variant >= 8) && b->prec == SCLBM_FP64)
         return set_error(SCLBM_E_INVALID_ARGUMENT,
                          "the load-ahead, compacted and uniform tile lists are for FP32/FP16 storage");
     b->use_units = variant == 3 || (variant == 0 && b->auto_units);
@@ -259,6 +277,7 @@ int sclbm_batch_set_kernel(sclbm_batch *b, int variant)
               : variant == 6 ? BODY_COMPACT
               : variant == 8 ? BODY_UNIFORM
               : variant == 9 ? BODY_HALF
+              : variant == 10 ? BODY_WARP
               : variant == 0 ? b->auto_body
                              : BODY_TILE;
     for (auto &g : b->graph)
@@ -272,7 +291,7 @@ int sclbm_batch_set_kernel(sclbm_batch *b, int variant)
 int sclbm_batch_info(const sclbm_batch *b, int *ntiles, int *grid_ctas)
 {
     if (!b) return set_error(SCLBM_E_INVALID_ARGUMENT, "null batch");
-    if (ntiles) *ntiles = !b->use_units && b->body == BODY_HALF ? b->ntiles_half : b->ntiles;
+    if (ntiles) *ntiles = b->use_units ? b->ntiles : batch_ntiles(b);
     if (grid_ctas)
         *grid_ctas = b->use_units ? b->band_grid : (b->prec == SCLBM_FP64 ? b->grid : b->grid_body[b->body]);
     return SCLBM_OK;

@@ -103,6 +103,61 @@ __global__ void __launch_bounds__(BATCH_TX, (sizeof(T) == 8 ? 1 : 5))
         batch_half_loop<S, T, FLAGS, 2>(doms, tiles, ntiles, parity, s_rho[1], s_m[1], sa[1]);
 }
 
+// One-warp tiles: each warp of a 128-thread CTA walks its own 32-column tiles
+// (tiles 4c + w, 4c + w + 4g, ...) with its own density ring and argument
+// block; the row loop needs only warp synchronisation, so warps never wait on
+// one another (the ensemble's widths 64..512: 89 % of the lanes busy).
+constexpr int WARP_TX = 32;
+template <typename S, typename T, int FLAGS>
+__global__ void __launch_bounds__(BATCH_TX, (sizeof(T) == 8 ? 1 : 5))
+    k_batch2_warp(const Fused2Args<S, T> *__restrict__ doms, const TileRef *__restrict__ tiles,
+                  int ntiles, int parity)
+{
+    constexpr int NW = BATCH_TX / WARP_TX;
+    __shared__ V2<T> s_rho[NW][4][WARP_TX];
+    __shared__ uint8_t s_m[NW][4][WARP_TX];
+    __shared__ __align__(16) Fused2Args<S, T> sa[NW];
+    static_assert(sizeof(Fused2Args<S, T>) % 4 == 0, "argument block copied as words");
+    const int w = threadIdx.x / WARP_TX, lane = threadIdx.x % WARP_TX;
+    int loaded = -1;
+    for (int i = NW * blockIdx.x + w; i < ntiles; i += NW * gridDim.x) {
+        const TileRef tr = tiles[i];
+        const int key = 2 * tr.dom + parity;
+        if (key != loaded) {
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(doms + key);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(&sa[w]);
+            for (int k = lane; k < (int)(sizeof(Fused2Args<S, T>) / 4); k += WARP_TX) dst[k] = src[k];
+            __syncwarp();
+            loaded = key;
+        }
+        const bool down = ((tr.yb / sa[w].tile_y) & 1) != 0;
+        fused2_tile<S, T, WARP_TX, false, FLAGS, false, false, false, SYNC_WARP>(
+            sa[w], tr.xb, tr.yb, s_rho[w], s_m[w], down);
+        __syncwarp(); // the warp's ring and block are reused by its next tile
+    }
+}
+
+template <typename S, typename T>
+inline cudaError_t launch_batch_warp_t(const Fused2Args<S, T> *doms, const TileRef *tiles,
+                                       int ntiles, int parity, int grid, int flags, cudaStream_t s)
+{
+    if (flags & KF_SOLID)
+        k_batch2_warp<S, T, KF_FORCE | KF_SOLID | KF_UNIFORM><<<grid, BATCH_TX, 0, s>>>(doms, tiles,
+                                                                                      ntiles, parity);
+    else
+        k_batch2_warp<S, T, KF_FORCE><<<grid, BATCH_TX, 0, s>>>(doms, tiles, ntiles, parity);
+    return cudaGetLastError();
+}
+
+template <typename S, typename T> inline int batch_warp_blocks_per_sm_t()
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &n, k_batch2_warp<S, T, KF_FORCE | KF_SOLID | KF_UNIFORM>, BATCH_TX, 0) != cudaSuccess)
+        return 1;
+    return n;
+}
+
 template <typename S, typename T>
 inline cudaError_t launch_batch_half_t(const Fused2Args<S, T> *doms, const TileRef *tiles,
                                        int ntiles, int parity, int grid, int flags, cudaStream_t s)
@@ -160,7 +215,8 @@ enum BatchBody {
     BODY_COMPACT = 2,
     BODY_UNIFORM = 3,
     BODY_HALF = 4, // two 64-column tiles per CTA (k_batch2_half), its own tile list
-    BODY_COUNT = 5
+    BODY_WARP = 5, // one 32-column tile per warp (k_batch2_warp), its own tile list
+    BODY_COUNT = 6
 };
 cudaError_t launch_batch_fp64(const Fused2Args<double, double> *doms, const TileRef *tiles,
                               int ntiles, int parity, int grid, int flags, cudaStream_t s);

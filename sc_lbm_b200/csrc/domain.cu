@@ -230,8 +230,7 @@ int domain_default_tile_y(const sclbm_domain *d)
     // resident 128-thread CTAs per SM: 6 for the FP32-arithmetic kernels (80
     // registers), 5 for their uniform solid form (96), 3 for FP64 (168)
     const bool uniform = d->has_solid && d->prec != SCLBM_FP64 && (d->variant == 0 || d->variant == 8);
-    const long per_sm = d->tx == 64 ? (d->prec == SCLBM_FP64 ? 6 : 10)
-                                    : (d->prec == SCLBM_FP64 ? 3 : (uniform ? 5 : 6));
+    const long per_sm = (d->prec == SCLBM_FP64 ? 3 : (uniform ? 5 : 6)) * (128 / d->tx);
     const long R = per_sm * sm_count();
     auto tiles = [&](long ty) { return tiles_x * (((long)d->ny + ty - 1) / ty); };
     if (tiles(base) >= 8 * R) return (int)base;
@@ -465,8 +464,8 @@ int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y)
 int sclbm_domain_set_threads(sclbm_domain *d, int tx)
 {
     if (!d) return set_error(SCLBM_E_INVALID_ARGUMENT, "null domain");
-    if (tx != 64 && tx != 128)
-        return set_error(SCLBM_E_INVALID_ARGUMENT, "threads per tile must be 64 or 128");
+    if (tx != 32 && tx != 64 && tx != 128)
+        return set_error(SCLBM_E_INVALID_ARGUMENT, "threads per tile must be 32, 64 or 128");
     d->tx = tx;
     return SCLBM_OK;
 }

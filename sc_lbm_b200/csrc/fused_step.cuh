@@ -613,10 +613,19 @@ __device__ __forceinline__ void fused2_tile_compact(const Fused2Args<S, T> &a, c
 // barrier BAR = 1, 2, ...; TX a multiple of 32, each warp in one part).  The
 // barrier number is an immediate: a register operand makes ptxas reserve all
 // sixteen barriers of the CTA, which caps residency at four CTAs per SM.
+// BAR = SYNC_WARP: the tile is one warp (TX = 32), which needs no barrier
+// beyond the warp's own.
+constexpr int SYNC_WARP = -1;
 template <int TX, int BAR> __device__ __forceinline__ void tile_sync()
 {
-    if constexpr (BAR == 0) __syncthreads();
-    else asm volatile("bar.sync %0, %1;" ::"n"(BAR), "n"(TX) : "memory");
+    if constexpr (BAR == SYNC_WARP) {
+        static_assert(TX == 32, "warp tiles are 32 columns wide");
+        __syncwarp();
+    } else if constexpr (BAR == 0) {
+        __syncthreads();
+    } else {
+        asm volatile("bar.sync %0, %1;" ::"n"(BAR), "n"(TX) : "memory");
+    }
 }
 
 template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS, bool PF = false,
@@ -735,14 +744,15 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
 // fits 80 registers (six CTAs) with two row buffers and 102 (five) with the
 // third buffer of the load-ahead form or the uniform solid form; FP64 is left
 // uncapped
-template <typename T, bool AHEAD, int FLAGS = 0> constexpr int fused_min_ctas()
+template <typename T, bool AHEAD, int FLAGS = 0, int TX = 128> constexpr int fused_min_ctas()
 {
-    return sizeof(T) == 8 ? 1 : (AHEAD || (FLAGS & KF_UNIFORM) ? 5 : 6);
+    // the same registers per thread for narrower tiles: proportionally more CTAs
+    return sizeof(T) == 8 ? 1 : (AHEAD || (FLAGS & KF_UNIFORM) ? 5 : 6) * (128 / TX);
 }
 
 template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS, bool PF = false,
           bool AHEAD = false, bool COMPACT = false, bool WIDE = false>
-__global__ void __launch_bounds__(TX, (fused_min_ctas<T, AHEAD, FLAGS>()))
+__global__ void __launch_bounds__(TX, (fused_min_ctas<T, AHEAD, FLAGS, TX>()))
     k_fused2(const __grid_constant__ Fused2Args<S, T> a)
 {
     __shared__ V2<T> s_rho[4][TX];
@@ -903,6 +913,11 @@ inline cudaError_t launch_fused2_any(const Fused2Args<S, T> &a, int variant, int
         return launch_fused2_f<S, T, 128, false, KF_FORCE | KF_SOLID, false, false, false, true>(a, s);
     const bool two = variant == 1;
     if (tx == 64) return launch_fused2_tx<S, T, 64>(a, two, s);
+    if (tx == 32) {
+        // one-warp tiles (no CTA barrier); variant 8: with the uniform solid form
+        if (variant == 8) return launch_fused2_tx<S, T, 32, false, false, false, KF_UNIFORM>(a, false, s);
+        return launch_fused2_tx<S, T, 32>(a, two, s);
+    }
     if (variant == 4) return launch_fused2_tx<S, T, 128, true>(a, false, s);
     if (variant == 5) return launch_fused2_tx<S, T, 128, false, true>(a, false, s);
     if (variant == 8) return launch_fused2_tx<S, T, 128, false, false, false, KF_UNIFORM>(a, false, s);

@@ -55,6 +55,8 @@ cudaError_t launch_batch_f32(const Fused2Args<float, float> *doms, const TileRef
                                                                  flags, s);
     if (body == BODY_HALF)
         return launch_batch_half_t<float, float>(doms, tiles, ntiles, parity, grid, flags, s);
+    if (body == BODY_WARP)
+        return launch_batch_warp_t<float, float>(doms, tiles, ntiles, parity, grid, flags, s);
     return launch_batch_t<float, float>(doms, tiles, ntiles, parity, grid, flags, s);
 }
 cudaError_t launch_batch_f16(const Fused2Args<__half, float> *doms, const TileRef *tiles,
@@ -69,6 +71,8 @@ cudaError_t launch_batch_f16(const Fused2Args<__half, float> *doms, const TileRe
                                                                  flags, s);
     if (body == BODY_HALF)
         return launch_batch_half_t<__half, float>(doms, tiles, ntiles, parity, grid, flags, s);
+    if (body == BODY_WARP)
+        return launch_batch_warp_t<__half, float>(doms, tiles, ntiles, parity, grid, flags, s);
     return launch_batch_t<__half, float>(doms, tiles, ntiles, parity, grid, flags, s);
 }
 int batch_blocks_per_sm_fp64();
@@ -81,12 +85,14 @@ int batch_blocks_per_sm(sclbm_precision p, int body)
                : body == BODY_COMPACT ? batch_blocks_per_sm_t<float, float, false, true>()
                : body == BODY_UNIFORM ? batch_blocks_per_sm_t<float, float, false, false, KF_UNIFORM>()
                : body == BODY_HALF    ? batch_half_blocks_per_sm_t<float, float>()
+               : body == BODY_WARP    ? batch_warp_blocks_per_sm_t<float, float>()
                                       : batch_blocks_per_sm_t<float, float>();
     default:
         return body == BODY_AHEAD     ? batch_blocks_per_sm_t<__half, float, true>()
                : body == BODY_COMPACT ? batch_blocks_per_sm_t<__half, float, false, true>()
                : body == BODY_UNIFORM ? batch_blocks_per_sm_t<__half, float, false, false, KF_UNIFORM>()
                : body == BODY_HALF    ? batch_half_blocks_per_sm_t<__half, float>()
+               : body == BODY_WARP    ? batch_warp_blocks_per_sm_t<__half, float>()
                                       : batch_blocks_per_sm_t<__half, float>();
     }
 }

@@ -72,7 +72,7 @@ def test_domain_fp64_bit_exact(sclbm, name):
                                                (64, 64, 1), (128, 0, 0), (128, 0, 3), (128, 0, 4),
                                                (128, 3, 4), (128, 0, 5), (128, 4, 5),
                                                (128, 0, 7), (128, 0, 8), (128, 3, 8),
-                                               (128, 0, 9)])
+                                               (128, 0, 9), (32, 0, 2), (32, 5, 8), (32, 4, 1)])
 def test_domain_fp64_tiling_invariant(sclbm, tx, tile_y, variant):
     """Kernel variant (pipelined persistent, two pass, register tile, register
     tile with L2 prefetch) and tile shape do not change a single bit."""
@@ -146,17 +146,20 @@ def test_shifted_forms_density_error(sclbm, oracle, name, steps, prec, tol_max, 
         assert e_max <= tol_max and e_l2 <= tol_l2, (name, prec, c, e_max, e_l2)
 
 
-@pytest.mark.parametrize("variant,tile_y", [(1, 4), (4, 0), (4, 7), (3, 0), (5, 0), (5, 7),
-                                            (5, 1), (5, 2), (6, 0), (6, 1), (6, 5), (6, 64),
-                                            (7, 0), (7, 3), (8, 0), (8, 5), (9, 0)])
-def test_shifted_variants_match_register_tile(sclbm, variant, tile_y):
-    """The shifted forms give the same bytes with every kernel variant."""
+@pytest.mark.parametrize("variant,tile_y,tx", [(1, 4, 128), (4, 0, 128), (4, 7, 128), (3, 0, 128),
+                                               (5, 0, 128), (5, 7, 128), (5, 1, 128), (5, 2, 128),
+                                               (6, 0, 128), (6, 1, 128), (6, 5, 128), (6, 64, 128),
+                                               (7, 0, 128), (7, 3, 128), (8, 0, 128), (8, 5, 128),
+                                               (9, 0, 128), (0, 0, 32), (2, 3, 32), (8, 7, 32)])
+def test_shifted_variants_match_register_tile(sclbm, variant, tile_y, tx):
+    """The shifted forms give the same bytes with every kernel variant and
+    tile width."""
     for prec in (sclbm.FP32_SHIFTED, sclbm.FP16_SHIFTED):
         if variant == 3 and prec == sclbm.FP16_SHIFTED:
             continue
         a = gpu_runner.run_domain(sclbm, RUNS["porous_96x48"], prec, rho_ref=(0.5, 1.5))
         b = gpu_runner.run_domain(sclbm, RUNS["porous_96x48"], prec, rho_ref=(0.5, 1.5),
-                                  variant=variant, tile_y=tile_y)
+                                  variant=variant, tile_y=tile_y, tx=tx)
         assert a["c1_f"].tobytes() == b["c1_f"].tobytes()
         assert a["c2_f"].tobytes() == b["c2_f"].tobytes()
 
@@ -209,7 +212,8 @@ def test_batch_matches_individual_domains(sclbm):
                                 (sclbm.FP16_SHIFTED, False, 5), (sclbm.FP32_SHIFTED, True, 6),
                                 (sclbm.FP16_SHIFTED, False, 6), (sclbm.FP32_SHIFTED, True, 8),
                                 (sclbm.FP16_SHIFTED, True, 8), (sclbm.FP32_SHIFTED, True, 9),
-                                (sclbm.FP16_SHIFTED, False, 9)):
+                                (sclbm.FP16_SHIFTED, False, 9), (sclbm.FP32_SHIFTED, True, 10),
+                                (sclbm.FP16_SHIFTED, False, 10)):
         rr = (0.8, 1.2)
         solo = [gpu_runner.run_domain(sclbm, dict(RUNS[n], steps=45), prec, rho_ref=rr) for n in names]
         doms = [gpu_runner.make_domain(sclbm, RUNS[n], prec, rho_ref=rr) for n in names]

@@ -204,8 +204,11 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
     // FP16 form has no band kernel)
     b->auto_units = b->prec != SCLBM_FP16_SHIFTED && nodes_units > nodes_tiles;
     // FP32/FP16 tile lists with solid nodes: the uniform solid body (512-domain
-    // ensemble, FP32: 21.7 vs 19.6 GLUPS)
-    b->auto_body = (b->flags & KF_SOLID) && b->prec != SCLBM_FP64 ? BODY_UNIFORM : BODY_TILE;
+    // ensemble, FP32: 21.7 vs 19.6 GLUPS), on one-warp tiles for FP16 storage
+    // (25.3 vs 23.5 GLUPS)
+    b->auto_body = !(b->flags & KF_SOLID) || b->prec == SCLBM_FP64 ? BODY_TILE
+                   : b->prec == SCLBM_FP16_SHIFTED                 ? BODY_WARP
+                                                                   : BODY_UNIFORM;
     b->body = b->auto_body;
     b->use_units = b->auto_units;
     std::vector<BandTile> bands;

@@ -337,17 +337,32 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
                     uy = fmaf(Fy[k], ir, ucy);
                 }
             }
+            // BGK toward the shifted equilibrium w_i (drho + rho poly_i),
+            // poly_i = 3 c.u + 4.5 (c.u)^2 - 1.5 u^2, written as
+            // d*_i = (1 - omega) d_i + w_i (omega rho poly_i + omega drho); the
+            // directions i and opp(i) share 4.5 (c.u)^2 - 1.5 u^2
             const float usq15 = 1.5f * fmaf(ux, ux, uy * uy);
-            const float om = a.c[k].omega;
+            const float om = a.c[k].omega, omm = a.c[k].one_m_omega;
+            const float am = om * r[k], bm = om * dr[k];
+            const float ux45 = 4.5f * ux, uy45 = 4.5f * uy;
+            float v[9];
+            v[0] = fmaf(float(w_eq(0)), fmaf(am, -usq15, bm), omm * float(f[k][0]));
+            auto pair = [&](int i, int j, float cu, float cu45) {
+                const float sq = fmaf(cu45, cu, -usq15);
+                v[i] = fmaf(float(w_eq(i)), fmaf(am, fmaf(3.f, cu, sq), bm), omm * float(f[k][i]));
+                v[j] = fmaf(float(w_eq(j)), fmaf(am, fmaf(-3.f, cu, sq), bm), omm * float(f[k][j]));
+            };
+            pair(1, 3, ux, ux45);                  // c = (+-1, 0)
+            pair(2, 4, uy, uy45);                  // c = (0, +-1)
+            pair(5, 7, ux + uy, ux45 + uy45);      // c = +-(1, 1)
+            pair(6, 8, uy - ux, uy45 - ux45);      // c = +-(-1, 1)
 #pragma unroll
             for (int i = 0; i < 9; ++i) {
-                const float fe = feq_dev(i, dr[k], r[k], ux, uy, usq15);
-                const T fi = f[k][i];
-                float v = fmaf(om, fe - fi, fi);
+                float vi = v[i];
                 // the force vector is zero for a component without a volume force
-                if constexpr (FORCE) v += a.c[k].force[i];
-                if constexpr (UNIFORM) v = self_fluid ? v : 0.f;
-                push_one<S, T, SOLID, WIDE>(a, k, i, v, nf[i], n);
+                if constexpr (FORCE) vi += a.c[k].force[i];
+                if constexpr (UNIFORM) vi = self_fluid ? vi : 0.f;
+                push_one<S, T, SOLID, WIDE>(a, k, i, vi, nf[i], n);
             }
         }
     }

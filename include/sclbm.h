@@ -254,9 +254,8 @@ int sclbm_domain_step(sclbm_domain *d, int nsteps);
  * FP64 (out[3*comp + 0..2]); out[6] = number of non-finite populations. */
 int sclbm_domain_mass_momentum(sclbm_domain *d, double out[7]);
 /* Kernel selection (all variants give identical results):
- *   0 = automatic (default): the fastest measured form -- on lattices with
- *       solid nodes 3 for FP64 storage and 8 for FP32/FP16 storage, 2 on
- *       all-fluid lattices;
+ *   0 = automatic (default): the fastest measured form -- 8 for FP32/FP16
+ *       storage on lattices with solid nodes, 2 otherwise;
  *   1 = two pass (density kernel, then the fused kernel reading it);
  *   2 = single pass, one tile per CTA, population rows held in registers;
  *   3 = single pass, population rows staged through a shared-memory ring by

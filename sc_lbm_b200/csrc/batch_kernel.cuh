@@ -20,10 +20,12 @@ struct TileRef {
 // registers.
 // Five resident CTAs per SM (102 registers): the tile loop and the shared
 // argument block leave the six-CTA cap of the single-domain kernel spilling,
-// and on the 512-domain ensemble the five-CTA form ran 13 % faster.
+// and on the 512-domain ensemble the five-CTA form ran 13 % faster.  FP64:
+// three CTAs per SM (168 registers, no spills; uncapped it took 174 and ran
+// two).
 template <typename S, typename T, int FLAGS = KF_FORCE | KF_SOLID, bool AHEAD = false,
           bool COMPACT = false>
-__global__ void __launch_bounds__(BATCH_TX, (sizeof(T) == 8 ? 1 : 5))
+__global__ void __launch_bounds__(BATCH_TX, (sizeof(T) == 8 ? 3 : 5))
     k_batch2(const Fused2Args<S, T> *__restrict__ doms, const TileRef *__restrict__ tiles,
              int ntiles, int parity)
 {
@@ -89,7 +91,7 @@ __device__ __forceinline__ void batch_half_loop(const Fused2Args<S, T> *__restri
 }
 
 template <typename S, typename T, int FLAGS>
-__global__ void __launch_bounds__(BATCH_TX, (sizeof(T) == 8 ? 1 : 5))
+__global__ void __launch_bounds__(BATCH_TX, (sizeof(T) == 8 ? 3 : 5))
     k_batch2_half(const Fused2Args<S, T> *__restrict__ doms, const TileRef *__restrict__ tiles,
                   int ntiles, int parity)
 {
@@ -109,7 +111,7 @@ __global__ void __launch_bounds__(BATCH_TX, (sizeof(T) == 8 ? 1 : 5))
 // one another (the ensemble's widths 64..512: 89 % of the lanes busy).
 constexpr int WARP_TX = 32;
 template <typename S, typename T, int FLAGS>
-__global__ void __launch_bounds__(BATCH_TX, (sizeof(T) == 8 ? 1 : 5))
+__global__ void __launch_bounds__(BATCH_TX, (sizeof(T) == 8 ? 3 : 5))
     k_batch2_warp(const Fused2Args<S, T> *__restrict__ doms, const TileRef *__restrict__ tiles,
                   int ntiles, int parity)
 {

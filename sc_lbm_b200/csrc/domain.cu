@@ -320,12 +320,11 @@ static cudaError_t step_one(const sclbm_domain *d, cudaStream_t s)
         if (e != cudaSuccess) return e;
     }
     // variant 0 picks the fastest measured form on B200: the register tile,
-    // with the uniform solid form where the lattice has solid nodes, except for
-    // FP64 storage on a lattice with solid nodes, where the pipelined kernel is
-    // faster (4096^2: 16.98 vs 16.55 GLUPS all-fluid; 14.8 vs 11.1 at 60 %
-    // fluid); 3 forces the pipelined kernel
-    const bool pipelined = d->variant == 3 || d->variant == 9 ||
-                           (d->variant == 0 && sizeof(S) == 8 && d->has_solid);
+    // with the uniform solid form where FP32/FP16 lattices have solid nodes
+    // (FP64 at 4096^2: register tile 17.4 GLUPS all-fluid, 15.4 at 60 % fluid,
+    // against 16.4 and 14.8 for the pipelined kernel); 3 and 9 force the
+    // pipelined kernel
+    const bool pipelined = d->variant == 3 || d->variant == 9;
     if (pipelined) {
         const bool uni = d->variant == 9;
         if constexpr (sizeof(S) == 8) return launch_fused2_async_fp64(a, s, uni);
@@ -335,9 +334,10 @@ static cudaError_t step_one(const sclbm_domain *d, cudaStream_t s)
     // tile with the uniform solid form; variant 2 (and the FP16 form):
     // register-tile single pass
     int v = d->variant == 1 || d->variant >= 4 ? d->variant : 0;
-    // variant 0 on a lattice with solid nodes: the uniform solid form
-    // (4096^2 FP32 at 60 % fluid: 29.7 vs 24.0 GLUPS; FP16 36.3 vs 32.7)
-    if (d->variant == 0 && d->has_solid) v = 8;
+    // variant 0 on an FP32/FP16 lattice with solid nodes: the uniform solid
+    // form (4096^2 FP32 at 60 % fluid: 29.7 vs 24.0 GLUPS; FP16 36.3 vs 32.7;
+    // FP64 runs it slower, 13.9 vs 15.4)
+    if (d->variant == 0 && d->has_solid && sizeof(S) != 8) v = 8;
     if constexpr (sizeof(S) == 8) return launch_fused2_fp64(a, v, d->tx, s);
     else if constexpr (sizeof(S) == 4) return launch_fused2_f32(a, v, d->tx, s);
     else return launch_fused2_f16(a, v, d->tx, s);

@@ -757,12 +757,13 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
 
 // resident 128-thread CTAs per SM the register cap aims at: FP32 arithmetic
 // fits 80 registers (six CTAs) with two row buffers and 102 (five) with the
-// third buffer of the load-ahead form or the uniform solid form; FP64 is left
-// uncapped
+// third buffer of the load-ahead form or the uniform solid form; FP64 fits
+// 168 (three CTAs) without spills -- uncapped, its solid forms took 178 and
+// ran two CTAs per SM
 template <typename T, bool AHEAD, int FLAGS = 0, int TX = 128> constexpr int fused_min_ctas()
 {
     // the same registers per thread for narrower tiles: proportionally more CTAs
-    return sizeof(T) == 8 ? 1 : (AHEAD || (FLAGS & KF_UNIFORM) ? 5 : 6) * (128 / TX);
+    return (sizeof(T) == 8 ? 3 : (AHEAD || (FLAGS & KF_UNIFORM) ? 5 : 6)) * (128 / TX);
 }
 
 template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS, bool PF = false,

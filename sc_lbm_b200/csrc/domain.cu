@@ -228,9 +228,11 @@ int domain_default_tile_y(const sclbm_domain *d)
     const long tiles_x = (long)((d->nx + W - 1) / W);
     const long base = d->prec == SCLBM_FP16_SHIFTED ? 32 : 16;
     // resident 128-thread CTAs per SM: 6 for the FP32-arithmetic kernels (80
-    // registers), 5 for their uniform solid form (96), 3 for FP64 (168)
+    // registers), 5 for their uniform solid form (96), 3 for FP64 (168), 4 for
+    // its all-fluid form without a volume force (128)
     const bool uniform = d->has_solid && d->prec != SCLBM_FP64 && (d->variant == 0 || d->variant == 8);
-    const long per_sm = (d->prec == SCLBM_FP64 ? 3 : (uniform ? 5 : 6)) * (128 / d->tx);
+    const bool plain = !d->has_solid && !d->p.force_on[0] && !d->p.force_on[1];
+    const long per_sm = (d->prec == SCLBM_FP64 ? (plain ? 4 : 3) : (uniform ? 5 : 6)) * (128 / d->tx);
     const long R = per_sm * sm_count();
     auto tiles = [&](long ty) { return tiles_x * (((long)d->ny + ty - 1) / ty); };
     if (tiles(base) >= 8 * R) return (int)base;

@@ -759,11 +759,12 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
 // fits 80 registers (six CTAs) with two row buffers and 102 (five) with the
 // third buffer of the load-ahead form or the uniform solid form; FP64 fits
 // 168 (three CTAs) without spills -- uncapped, its solid forms took 178 and
-// ran two CTAs per SM
+// ran two CTAs per SM -- and its all-fluid form 128 (four CTAs)
 template <typename T, bool AHEAD, int FLAGS = 0, int TX = 128> constexpr int fused_min_ctas()
 {
     // the same registers per thread for narrower tiles: proportionally more CTAs
-    return (sizeof(T) == 8 ? 3 : (AHEAD || (FLAGS & KF_UNIFORM) ? 5 : 6)) * (128 / TX);
+    return (sizeof(T) == 8 ? (FLAGS == 0 && !AHEAD ? 4 : 3) : (AHEAD || (FLAGS & KF_UNIFORM) ? 5 : 6)) *
+           (128 / TX);
 }
 
 template <typename S, typename T, int TX, bool TWO_PASS, int FLAGS, bool PF = false,

@@ -6,8 +6,9 @@ device domain does) and packs / unpacks halo rows in the library's buffer
 layout.  After n steps with halos exchanged every k steps, the owned rows of
 every slab must equal, bit for bit, the oracle run on the whole lattice:
 * three slabs of uneven heights in one process (LocalRing over host buffers);
-* two ranks over gloo (DistRing, world size 2: the two transfers to the same
-  peer are told apart by their tags), and one rank exchanging with itself.
+* ranks over gloo (DistRing): world size 2 (the two transfers to the same
+  peer are told apart by their tags), 3 (distinct neighbours), and one rank
+  exchanging with itself.
 Porous lattice with walls, both solid interactions and a volume force.
 """
 import ctypes
@@ -150,7 +151,7 @@ def _worker(rank, world, port, steps, k, q):
     q.put((rank, ok))
 
 
-@pytest.mark.parametrize("world", [1, 2])
+@pytest.mark.parametrize("world", [1, 2, 3])
 def test_dist_ring_gloo(world):
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")

@@ -135,6 +135,15 @@ class DistRing:
         nb = slab.halo_bytes()
         self.bufs = {k: torch.empty(nb, dtype=torch.uint8, device=device)
                      for k in ("send_low", "send_up", "recv_low", "recv_up")}
+        self.torch = torch
+        self.cuda = torch.device(device).type == "cuda"
+
+    def _library_stream(self):
+        """The stream the library queues its copies on (torch's own streams
+        order the transfers): each waits for the other around the exchange."""
+        from .capi import lib
+        ptr = lib().sclbm_get_stream()
+        return self.torch.cuda.ExternalStream(ptr) if ptr else None
 
     def _peer(self, r):
         g = r % self.world
@@ -144,6 +153,9 @@ class DistRing:
         b, s = self.bufs, self.slab
         s.pack(0, b["send_low"].data_ptr())
         s.pack(1, b["send_up"].data_ptr())
+        lib_stream = self._library_stream() if self.cuda else None
+        if lib_stream is not None:
+            self.torch.cuda.current_stream().wait_stream(lib_stream)
         if self.world == 1:
             b["recv_low"].copy_(b["send_up"])
             b["recv_up"].copy_(b["send_low"])
@@ -156,6 +168,8 @@ class DistRing:
                    d.P2POp(d.irecv, b["recv_low"], prev, self.group, 1)]
             for req in d.batch_isend_irecv(ops):
                 req.wait()
+        if lib_stream is not None:
+            lib_stream.wait_stream(self.torch.cuda.current_stream())
         s.unpack(0, b["recv_low"].data_ptr())
         s.unpack(1, b["recv_up"].data_ptr())
 

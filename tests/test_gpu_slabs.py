@@ -6,6 +6,7 @@
   (FP64 therefore bit-identical to the reference), on a porous lattice with
   walls, solid interactions and a volume force;
 * the halo entry points refuse bad arguments;
+* a one-rank NCCL ring on the library's own stream equals the whole lattice;
 * the torchrun driver (one rank, NCCL process group, the exchange with
   itself) runs and reports its line.
 """
@@ -56,6 +57,33 @@ def test_slabs_on_one_gpu_match_whole_lattice(sclbm, prec_name, k):
         w = whole.download_f(c).reshape(9, ny, nx)
         for s, (y0, y1) in zip(ss, cuts):
             assert s.owned_f(c).tobytes() == np.ascontiguousarray(w[:, y0:y1, :]).tobytes(), (y0, c)
+
+
+def test_dist_ring_one_rank_nccl_on_the_library_stream(sclbm, tmp_path):
+    """DistRing over an NCCL group of one rank while the library keeps its own
+    stream (no set_stream): the exchange orders the library's copies and
+    torch's stream, and the slab equals the whole lattice byte for byte."""
+    import torch
+    import torch.distributed as dist
+    from sc_lbm_b200 import slabs
+    nx, ny, m, p, f1, f2 = _lattice(sclbm)
+    whole = sclbm.Domain(nx, ny, m, p, sclbm.FP32_SHIFTED)
+    whole.upload_f(0, f1)
+    whole.upload_f(1, f2)
+    whole.step(9)
+    store = dist.FileStore(str(tmp_path / "store"), 1)
+    dist.init_process_group("nccl", store=store, rank=0, world_size=1,
+                            device_id=torch.device("cuda", 0))
+    try:
+        s = slabs.Slab(nx, ny, m, 0, ny, 2, params=p, precision=sclbm.FP32_SHIFTED)
+        s.upload_f(0, f1)
+        s.upload_f(1, f2)
+        slabs.run([s], slabs.DistRing(s), 9)
+        torch.cuda.synchronize()
+        for c in range(2):
+            assert s.owned_f(c).tobytes() == whole.download_f(c).tobytes()
+    finally:
+        dist.destroy_process_group()
 
 
 def test_halo_arguments(sclbm):

@@ -1,6 +1,7 @@
 """The numpy restatement of the reference's contact-angle script
 (oracle/post.py) against what the unmodified script printed on the same
-synthetic fields (tests/golden/contact_angle_golden.json, made by
+synthetic fields and on the reduced benchmark's density files written by the
+compiled reference (tests/golden/contact_angle_golden.json, made by
 make_contact_angle_golden.py), its failure cases, and the contact-angle
 workload's initial state against the oracle's rectangle initialiser (CPU).
 """
@@ -60,3 +61,17 @@ def test_contact_workload_matches_reference_initialiser(sclbm, oracle):
     assert np.array_equal(w["f1"], r["c1_f"])
     assert np.array_equal(w["f2"], r["c2_f"])
     assert w["Gs"] == (0.3, -0.3)
+
+
+def test_reduced_benchmark_angle_matches_reference_text_route(oracle):
+    """The reduced contact-angle benchmark (golden case contact_120x90): the
+    restatement on the oracle's final densities (bit-identical to the compiled
+    reference's) gives the angle the reference's script printed on the density
+    files the reference itself wrote in six-digit text."""
+    import cases
+    with open(GOLDEN) as fh:
+        want = json.load(fh)["reduced_benchmark"]
+    case = cases.all_cases()[want["case"]]
+    r = oracle.run_case(case)
+    got = post.contact_angle(r["c1_rho_final"], r["c2_rho_final"], case["nx"], case["ny"])
+    assert got["theta"] == want["theta_deg"]

@@ -3,11 +3,14 @@ INFRASTRUCTURE ONLY): the checkers of the library's on-device measurements.
 
 * ``contact_angle`` -- benchmarks/two_phase_two_components_flows/
   contact_angles/compute_contact_angles.py:45-106, on density fields held in
-  memory instead of the loaded text files.
+  memory instead of the loaded text files;
+* ``laplace`` -- benchmarks/two_phase_two_components_flows/laplace_law/
+  compute_surface_tension.py:64-72 (pressure jump and radius of one droplet).
 
-Pinned against the script itself: tests/golden/make_contact_angle_golden.py
-runs the unmodified script on seeded synthetic fields and records what it
-prints (tests/golden/contact_angle_golden.json).
+Pinned against the scripts themselves: tests/golden/make_contact_angle_golden.py
+and tests/golden/make_laplace_golden.py run the unmodified scripts on seeded
+synthetic fields and record what they compute
+(tests/golden/contact_angle_golden.json, tests/golden/laplace_golden.json).
 """
 from __future__ import annotations
 
@@ -60,3 +63,26 @@ def contact_angle(rho_b: np.ndarray, rho_d: np.ndarray, nx: int, ny: int,
         theta += 180
     return {"theta": theta, "L": L, "H": H, "R": R, "xL": xL, "xR": xR, "y_min": y2,
             "y_max": int(ys.max()), "band_nodes": int(ys.size)}
+
+
+def laplace(rho_b: np.ndarray, rho_d: np.ndarray, nx: int, ny: int, G: float = 0.9,
+            p_in=(200, 200), p_out=(370, 370), rho_bulk: float = 1.9,
+            rho_disp: float = 0.06) -> dict:
+    """Pressure jump and radius of a droplet (density rho_d) in the bulk fluid.
+
+    p = (rho_b + rho_d)/3 + G/3 rho_b rho_d (compute_surface_tension.py:65),
+    dp = p[p_in] - p[p_out] with the points given as [row, column] (:66), the
+    radius as half the row extent and half the column extent of the band
+    rho_d - rho_b < 0, rho_disp < rho_b <= rho_bulk, averaged (:69-72).
+    """
+    rb = np.asarray(rho_b, dtype=np.float64).reshape(ny, nx)
+    rd = np.asarray(rho_d, dtype=np.float64).reshape(ny, nx)
+    p = 1.0 / 3.0 * (rb + rd) + G / 3.0 * rb * rd
+    dp = p[p_in[0], p_in[1]] - p[p_out[0], p_out[1]]
+    sel = np.where((rd - rb < 0) & (rb <= rho_bulk) & (rb > rho_disp))
+    if sel[0].size == 0:
+        raise ValueError("no interface nodes")
+    Rx = (np.amax(sel[0]) - np.amin(sel[0])) / 2.0
+    Ry = (np.amax(sel[1]) - np.amin(sel[1])) / 2.0
+    return {"dp": float(dp), "R": float(0.5 * (Rx + Ry)), "R_rows": float(Rx), "R_cols": float(Ry),
+            "band_nodes": int(sel[0].size)}

@@ -5,12 +5,15 @@ INFRASTRUCTURE ONLY): the checkers of the library's on-device measurements.
   contact_angles/compute_contact_angles.py:45-106, on density fields held in
   memory instead of the loaded text files;
 * ``laplace`` -- benchmarks/two_phase_two_components_flows/laplace_law/
-  compute_surface_tension.py:64-72 (pressure jump and radius of one droplet).
+  compute_surface_tension.py:64-72 (pressure jump and radius of one droplet);
+* ``channel_profile``, ``velocity_stats`` -- scripts/benchmark_utils.py:8-60
+  (the analytic channel profile, the largest |u| and the mean nonzero |u|).
 
-Pinned against the scripts themselves: tests/golden/make_contact_angle_golden.py
-and tests/golden/make_laplace_golden.py run the unmodified scripts on seeded
-synthetic fields and record what they compute
-(tests/golden/contact_angle_golden.json, tests/golden/laplace_golden.json).
+Pinned against the scripts themselves: tests/golden/make_contact_angle_golden.py,
+tests/golden/make_laplace_golden.py and tests/golden/make_utils_golden.py run
+the unmodified scripts on seeded synthetic inputs and record what they compute
+(tests/golden/contact_angle_golden.json, laplace_golden.json,
+utils_golden.json).
 """
 from __future__ import annotations
 
@@ -86,3 +89,25 @@ def laplace(rho_b: np.ndarray, rho_d: np.ndarray, nx: int, ny: int, G: float = 0
     Ry = (np.amax(sel[1]) - np.amin(sel[1])) / 2.0
     return {"dp": float(dp), "R": float(0.5 * (Rx + Ry)), "R_rows": float(Rx), "R_cols": float(Ry),
             "band_nodes": int(sel[0].size)}
+
+
+def channel_profile(nx: int, ny: int, dPdL: float, direction: str, mu: float):
+    """Analytic laminar profile between plates one node thick
+    (benchmark_utils.py:8-52): lateral node positions and u, the half width
+    h = (n_lat - 2)/2, u = u_max (1 - (y/h)^2), u_max = dPdL h^2 / (2 mu), and
+    a zero at each wall node."""
+    n_lat = ny if direction == "x" else nx
+    h = (n_lat - 2.0) / 2.0
+    u_max = dPdL * (h * h) / (2.0 * mu)
+    lat = np.arange(-h, h) + 0.5
+    u = u_max * (1.0 - (lat / h) * (lat / h))
+    return (np.concatenate([[lat[0] - 1], lat, [lat[-1] + 1]]),
+            np.concatenate([[0.0], u, [0.0]]))
+
+
+def velocity_stats(ux: np.ndarray, uy: np.ndarray) -> dict:
+    """Largest |u| and mean of the nonzero |u| (vel_mag and ave,
+    benchmark_utils.py:54-60)."""
+    m = np.sqrt(np.asarray(ux) * ux + np.asarray(uy) * uy).ravel()
+    nz = m[np.flatnonzero(m)]
+    return {"max_u": float(m.max()), "mean_nonzero_u": float(np.mean(nz)), "nonzero": int(nz.size)}

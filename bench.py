@@ -189,6 +189,16 @@ def run_reference(args):
         kind = "port"
     t = sum(per)
     mlups = nx * ny * len(per) / t / 1e6
+    # The reference is serial: one lattice runs on one core, which is the
+    # headline reference value.  For context, the whole host's throughput on
+    # independent lattices (one serial run per core, 512 x 512, 10 steps).
+    all_cores = None
+    if kind == "reference":
+        cores = max(1, min(os.cpu_count() or 1, 64))
+        par = pyoracle.ref_bench_parallel(512, 512, 10, cores)
+        all_cores = {"instances": cores, "value": round(par["mlups"], 3), "unit": "MLUPS",
+                     "sample": "independent 512x512 lattices, 10 steps each, one serial "
+                               "reference run per core at once"}
     line = {
         "metric": "two-component D2Q9 Shan-Chen step throughput", "value": round(mlups, 4),
         "unit": "MLUPS", "impl": "reference", "n_gpus": world, "steps": args.steps,
@@ -200,7 +210,8 @@ def run_reference(args):
                    "lattice_sample": [nx, ny], "precision": "fp64 (reference serial C++)"},
         "cpu_baseline": {"value": round(mlups, 4), "unit": "MLUPS", "cores": 1, "kind": kind,
                          "sample": f"{len(per)} steps of a {nx}x{ny} two-component periodic "
-                                   "lattice, reference call sequence laplace_law.cpp:123-133"},
+                                   "lattice, reference call sequence laplace_law.cpp:123-133",
+                         "all_cores": all_cores},
         "e2e": {"value": round(mlups, 4), "unit": "MLUPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "gpu_launches": 0,

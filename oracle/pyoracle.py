@@ -335,6 +335,26 @@ def run_ref(case, runner: str | None = None) -> dict:
         return read_ref_output(out_path)
 
 
+def ref_bench_parallel(nx: int, ny: int, steps: int, instances: int) -> dict:
+    """`instances` independent serial reference runs at once, one per core
+    (the reference code itself is single-threaded): aggregate lattice updates
+    per second over the wall time from the first start to the last finish."""
+    import json
+    import time
+    t0 = time.perf_counter()
+    procs = [subprocess.Popen([REF_RUNNER, "bench", str(nx), str(ny), str(steps), str(1 + k)],
+                              stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+             for k in range(instances)]
+    outs = [p.communicate()[0] for p in procs]
+    wall = time.perf_counter() - t0
+    if any(p.returncode for p in procs):
+        raise RuntimeError("reference bench run failed")
+    runs = [json.loads(o.strip().splitlines()[-1]) for o in outs]
+    return {"instances": instances, "wall_seconds": wall,
+            "mlups": instances * nx * ny * steps / wall / 1e6,
+            "per_instance_mlups": [r["mlups"] for r in runs]}
+
+
 def ref_bench(nx: int, ny: int, steps: int, seed: int = 1) -> dict:
     """Time the reference's serial two-component step (one core)."""
     import json

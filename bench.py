@@ -194,7 +194,8 @@ def run_reference(args):
     # independent lattices (one serial run per core, 512 x 512, 10 steps).
     all_cores = None
     if kind == "reference":
-        cores = max(1, min(os.cpu_count() or 1, 64))
+        usable = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+        cores = max(1, min(usable or 1, 64))
         par = pyoracle.ref_bench_parallel(512, 512, 10, cores)
         all_cores = {"instances": cores, "value": round(par["mlups"], 3), "unit": "MLUPS",
                      "sample": "independent 512x512 lattices, 10 steps each, one serial "

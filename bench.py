@@ -11,9 +11,13 @@ Inputs are generated from a seeded splitmix64 stream ("data": "synthetic").
 
 One JSON line is printed by rank 0.  Under torchrun each rank advances its own
 independent replica (weak scaling, no collective on the data path); the time
-is the max over ranks.  `--impl reference` times the reference's own serial
-CPU step (oracle/_ref, the unmodified library compiled from its sources; or,
-when that was not built, the C restatement in oracle/) on a bounded sample.
+is the max over ranks.  Without torchrun, `--gpus N` (N > 1) starts the N rank
+processes itself (RANK / LOCAL_RANK / WORLD_SIZE / MASTER_* set per process).
+`--impl reference` times the reference's own serial CPU step (oracle/_ref, the
+unmodified library compiled from its sources; or, when that was not built,
+the C restatement in oracle/) on the same 4096x4096 lattice, pinned to one
+core; it stops after a bounded time (at least three timed steps) and says how
+many steps it timed.
 """
 from __future__ import annotations
 
@@ -35,7 +39,8 @@ NX = NY = 4096
 G12 = 1.2
 B_LU = {"fp64": 36 * 8 + 1, "fp32s": 36 * 4 + 1, "fp16s": 36 * 2 + 1}  # bytes / lattice update
 E2E_STEPS = 100  # LBM steps per end-to-end call
-CPU_SAMPLE = (1024, 1024)  # reference CPU sample lattice (same per-node work)
+REF_BUDGET_S = 240.0  # reference arm: stop timing after this long (>= 3 timed steps)
+CPU_LEG_STEPS = (1, 3)  # our arm's CPU-baseline leg: warm-up and timed steps
 
 
 def env_rank():
@@ -173,20 +178,30 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # reference arm
 # ---------------------------------------------------------------------------
+def reference_steps(nx, ny, warmup, steps, budget_s):
+    """Per-step seconds of the reference's serial step on an nx x ny lattice,
+    pinned to one core: the compiled reference (oracle/_ref) when it was
+    built, else the C restatement.  Timing stops after budget_s seconds once
+    three steps past the warm-up have run.  Returns (seconds, kind, info)."""
+    from oracle import pyoracle
+    info = pyoracle.cpu_info()
+    if pyoracle.have_ref():
+        r = pyoracle.ref_bench(nx, ny, warmup + steps, core=info["pin_core"],
+                               max_seconds=budget_s, min_steps=warmup + min(3, steps))
+        return r["step_seconds"][warmup:], "reference", info
+    return cpu_port_steps(nx, ny, warmup + steps, info["pin_core"], budget_s,
+                          warmup + min(3, steps))[warmup:], "port", info
+
+
 def run_reference(args):
     rank, world, _ = env_rank()
+    check_world(args, world)
     if rank != 0:
         return
     from oracle import pyoracle
-    nx, ny = CPU_SAMPLE
-    steps = args.warmup + args.steps
-    if pyoracle.have_ref():
-        r = pyoracle.ref_bench(nx, ny, steps)
-        per = r["step_seconds"][args.warmup:]
-        kind = "reference"
-    else:
-        per = cpu_port_steps(nx, ny, steps)[args.warmup:]
-        kind = "port"
+    nx, ny = args.lattice
+    warm = min(args.warmup, 3)
+    per, kind, info = reference_steps(nx, ny, warm, args.steps, REF_BUDGET_S)
     t = sum(per)
     mlups = nx * ny * len(per) / t / 1e6
     # The reference is serial: one lattice runs on one core, which is the
@@ -194,25 +209,29 @@ def run_reference(args):
     # independent lattices (one serial run per core, 512 x 512, 10 steps).
     all_cores = None
     if kind == "reference":
-        usable = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
-        cores = max(1, min(usable or 1, 64))
+        cores = max(1, min(info["usable"], 64))
         par = pyoracle.ref_bench_parallel(512, 512, 10, cores)
         all_cores = {"instances": cores, "value": round(par["mlups"], 3), "unit": "MLUPS",
                      "sample": "independent 512x512 lattices, 10 steps each, one serial "
                                "reference run per core at once"}
+    same = (nx, ny) == (NX, NY)
     line = {
         "metric": "two-component D2Q9 Shan-Chen step throughput", "value": round(mlups, 4),
         "unit": "MLUPS", "impl": "reference", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(1e3 * t / len(per), 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"spinodal two-component {NX}x{NY} periodic, G12={G12}, "
-                               f"sampled on a {nx}x{ny} lattice (same per-node work)",
-                   "lattice_sample": [nx, ny], "precision": "fp64 (reference serial C++)"},
+        "config": {"workload": f"spinodal two-component {nx}x{ny} periodic, tau=1, G12={G12}, "
+                               "rho=1+-1% seeded" + ("" if same else " (reduced lattice)"),
+                   "lattice": [nx, ny], "precision": "fp64 (reference serial C++)",
+                   "timed_steps": len(per), "warmup_steps_run": warm,
+                   "time_budget_s": REF_BUDGET_S},
         "cpu_baseline": {"value": round(mlups, 4), "unit": "MLUPS", "cores": 1, "kind": kind,
-                         "sample": f"{len(per)} steps of a {nx}x{ny} two-component periodic "
-                                   "lattice, reference call sequence laplace_law.cpp:123-133",
-                         "all_cores": all_cores},
+                         "sample": f"{len(per)} steps of the {nx}x{ny} two-component periodic "
+                                   "lattice after " + f"{warm} warm-up steps, reference call "
+                                   "sequence laplace_law.cpp:123-133",
+                         "cpu_model": info["model"], "nproc": info["nproc"],
+                         "pinned_core": info["pin_core"], "all_cores": all_cores},
         "e2e": {"value": round(mlups, 4), "unit": "MLUPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "gpu_launches": 0,
@@ -220,10 +239,15 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def cpu_port_steps(nx, ny, steps):
-    """Per-step seconds of the C restatement (oracle/) -- the fallback CPU arm."""
+def cpu_port_steps(nx, ny, steps, core=None, budget_s=0.0, min_steps=1):
+    """Per-step seconds of the C restatement (oracle/) -- the fallback CPU arm
+    (this process pinned to `core` while it runs)."""
     import ctypes as C
     from oracle import pyoracle
+    old_aff = None
+    if core is not None and hasattr(os, "sched_setaffinity"):
+        old_aff = os.sched_getaffinity(0)
+        os.sched_setaffinity(0, {core})
     L = pyoracle.lib()
     N = nx * ny
     g = np.ones(N, np.uint8)
@@ -242,11 +266,16 @@ def cpu_port_steps(nx, ny, steps):
         comps.append(c)
     tmp = np.zeros(9 * N)
     out = []
-    for _ in range(steps):
+    start = time.perf_counter()
+    for k in range(steps):
         t0 = time.perf_counter()
         L.orc_run_two(nx, ny, pyoracle._p(g), C.byref(comps[0]), C.byref(comps[1]), None, 0, 1,
                       pyoracle._p(tmp))
         out.append(time.perf_counter() - t0)
+        if budget_s > 0 and k + 1 >= min_steps and time.perf_counter() - start > budget_s:
+            break
+    if old_aff is not None:
+        os.sched_setaffinity(0, old_aff)
     return out
 
 
@@ -367,6 +396,7 @@ def run_ours(args):
     import sc_lbm_b200 as sc
 
     rank, world, local = env_rank()
+    check_world(args, world)
     torch.cuda.set_device(local)
     ranks = Ranks("nccl", "cuda")
     stream = torch.cuda.Stream()
@@ -432,22 +462,17 @@ def run_ours(args):
     e2e_s = max_over_ranks(time.perf_counter() - t0) / e2e_calls
     e2e_mlups = world * N * E2E_STEPS / e2e_s / 1e6
 
-    # --- CPU baseline (reference serial code on a bounded sample) -------------
+    # --- CPU baseline (reference serial code, same lattice, a few steps) -------
     cpu = None
     if rank == 0 and not args.no_cpu:
-        from oracle import pyoracle
-        nx, ny = CPU_SAMPLE
-        if pyoracle.have_ref():
-            r = pyoracle.ref_bench(nx, ny, 12)
-            per = r["step_seconds"][2:]
-            kind = "reference"
-        else:
-            per = cpu_port_steps(nx, ny, 6)[1:]
-            kind = "port"
-        cpu = {"value": round(nx * ny * len(per) / sum(per) / 1e6, 4), "unit": "MLUPS",
+        w, k = CPU_LEG_STEPS
+        per, kind, info = reference_steps(NX, NY, w, k, 60.0)
+        cpu = {"value": round(NX * NY * len(per) / sum(per) / 1e6, 4), "unit": "MLUPS",
                "cores": 1, "kind": kind,
-               "sample": f"{len(per)} steps of a {nx}x{ny} two-component periodic lattice "
-                         "(reference call sequence, same per-node work as the workload)"}
+               "sample": f"{len(per)} steps of the {NX}x{NY} two-component periodic lattice "
+                         f"after {w} warm-up step (reference call sequence "
+                         "laplace_law.cpp:123-133), one pinned core",
+               "cpu_model": info["model"], "nproc": info["nproc"], "pinned_core": info["pin_core"]}
 
     peak, peak_kind = measured_peak_hbm()
     achieved = B_LU["fp32s"] * N / (ms_step * 1e-3) / 1e9
@@ -489,6 +514,28 @@ def run_ours(args):
     ranks.close()
 
 
+def check_world(args, world):
+    if world != args.gpus:
+        raise SystemExit(f"bench.py --gpus {args.gpus} but {world} rank process(es) are running")
+
+
+def self_launch(argv, n):
+    """Start the n rank processes of `bench.py --gpus n` when no launcher did:
+    one process per GPU with RANK / LOCAL_RANK / WORLD_SIZE / MASTER_ADDR /
+    MASTER_PORT set, rank 0's output passed through; exit status = the worst."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    procs = []
+    for r in range(n):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(n),
+                   LOCAL_WORLD_SIZE=str(n), MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, os.path.abspath(__file__)] + argv, env=env))
+    rcs = [p.wait() for p in procs]
+    return max(abs(rc) for rc in rcs)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -497,8 +544,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-domain ensemble leg")
+    ap.add_argument("--lattice", type=int, nargs=2, default=[NX, NY], metavar=("NX", "NY"),
+                    help="reference arm only: a smaller lattice for quick checks (labelled)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(self_launch(sys.argv[1:], args.gpus))
     if args.impl == "reference":
         run_reference(args)
     else:

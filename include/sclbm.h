@@ -293,11 +293,17 @@ size_t sclbm_domain_device_bytes(const sclbm_domain *d);
  * file-scope device array (about 128 KB, held on every GPU that loads the
  * library until exit), which limits the lattice to 2^27 nodes (e.g.
  * 16384 x 8192); larger lattices return SCLBM_E_INVALID_ARGUMENT.  The first
- * call on a device looks up the array's device address, so make that first
- * call before any stream capture.  All calls share the array and it keeps
- * the last call's partial sums; calls that overlap on the GPU race.  Work
- * runs on `cuda_stream` (NULL = the default stream), which is synchronised
- * before out[7] (as sclbm_domain_mass_momentum) is returned. */
+ * call on a device looks up the array's device address and loads the
+ * monitor's kernels for all three precisions, so make one call on each
+ * device before entering a region where nothing may be allocated or loaded.
+ * All calls share the array and it keeps the last call's partial sums; calls
+ * that overlap on the GPU race.  Work runs on `cuda_stream` (NULL = the
+ * default stream), which is synchronised before out[7] (as
+ * sclbm_domain_mass_momentum) is returned; so it must not be called while
+ * that stream is being captured into a CUDA graph: a capturing stream is
+ * refused with SCLBM_E_INVALID_ARGUMENT before anything is enqueued, and the
+ * capture is left intact.  A non-finite population returns SCLBM_E_NONFINITE
+ * (out[6] holds the count). */
 int sclbm_mass_momentum_noalloc(const void *f0, const void *f1, const uint8_t *mask, size_t nx,
                                 size_t ny, int ncomp, int precision, const double *rho_ref,
                                 void *cuda_stream, double out[7]);

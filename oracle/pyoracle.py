@@ -355,9 +355,44 @@ def ref_bench_parallel(nx: int, ny: int, steps: int, instances: int) -> dict:
             "per_instance_mlups": [r["mlups"] for r in runs]}
 
 
-def ref_bench(nx: int, ny: int, steps: int, seed: int = 1) -> dict:
-    """Time the reference's serial two-component step (one core)."""
+def cpu_info() -> dict:
+    """The host's CPU model string, its logical CPU count and the CPUs this
+    process may run on (the first of them is the one serial runs pin to)."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for ln in fh:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    usable = sorted(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else \
+        list(range(os.cpu_count() or 1))
+    return {"model": model, "nproc": os.cpu_count(), "usable": len(usable), "pin_core": usable[0]}
+
+
+def _pinned(cmd, core):
+    """`cmd` pinned to one core: taskset -c <core> when present, else the
+    scheduler affinity set in the child before exec."""
+    import shutil
+    if core is None:
+        return cmd, None
+    if shutil.which("taskset"):
+        return ["taskset", "-c", str(core)] + cmd, None
+    return cmd, (lambda: os.sched_setaffinity(0, {core}))
+
+
+def ref_bench(nx: int, ny: int, steps: int, seed: int = 1, core=None, max_seconds: float = 0.0,
+              min_steps: int = 1) -> dict:
+    """Time the reference's serial two-component step on one core (`core`
+    pins it).  With max_seconds > 0 the run stops once that much time has
+    passed and at least min_steps steps are done; `step_seconds` lists the
+    steps that ran."""
     import json
-    r = subprocess.run([REF_RUNNER, "bench", str(nx), str(ny), str(steps), str(seed)],
-                       check=True, capture_output=True, text=True)
-    return json.loads(r.stdout.strip().splitlines()[-1])
+    cmd, pre = _pinned([REF_RUNNER, "bench", str(nx), str(ny), str(steps), str(seed),
+                        repr(float(max_seconds)), str(int(min_steps))], core)
+    r = subprocess.run(cmd, check=True, capture_output=True, text=True, preexec_fn=pre)
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    out["pinned_core"] = core
+    return out

@@ -10,7 +10,7 @@
 //   per operator  : tests/lbm/lbm_tests.cpp:12-44 and :119-127
 //
 // usage: sclbm_ref_runner case <spec.txt>      (writes the path named by `out`)
-//        sclbm_ref_runner bench <nx> <ny> <steps> <seed>
+//        sclbm_ref_runner bench <nx> <ny> <steps> <seed> [max_seconds min_steps]
 //        sclbm_ref_runner text <f.bin> <nx> <ny> <prefix>
 #include <chrono>
 #include <cstdint>
@@ -292,7 +292,9 @@ int run_case(const std::string &spec)
 
 // Serial timing of the reference two-component step (spinodal-type periodic
 // domain, rho = 1 +- 1% per component, G = 1.2, tau = 1), for the CPU baseline.
-int run_bench(size_t nx, size_t ny, int steps, unsigned seed)
+// Runs `steps` steps, or stops early once max_seconds (> 0) have passed and at
+// least min_steps steps are done (large lattices take seconds per step).
+int run_bench(size_t nx, size_t ny, int steps, unsigned seed, double max_seconds, int min_steps)
 {
     Geometry geom(nx, ny);
     LBM lbm(geom);
@@ -328,7 +330,11 @@ int run_bench(size_t nx, size_t ny, int steps, unsigned seed)
         lbm.collide(a, b);
         lbm.stream(geom, a, b);
         per_step.push_back(std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count());
+        if (max_seconds > 0.0 && k + 1 >= min_steps &&
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > max_seconds)
+            break;
     }
+    steps = (int)per_step.size();
     double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     double chk = 0.0;
     for (double x : a.get_f_dist()) chk += x;
@@ -367,7 +373,9 @@ int main(int argc, char **argv)
                         argv[5]);
     if (argc >= 5 && std::string(argv[1]) == "bench")
         return run_bench(std::strtoull(argv[2], 0, 10), std::strtoull(argv[3], 0, 10),
-                         std::atoi(argv[4]), argc > 5 ? (unsigned)std::atoi(argv[5]) : 1u);
-    std::fprintf(stderr, "usage: %s case <spec> | bench <nx> <ny> <steps> [seed]\n", argv[0]);
+                         std::atoi(argv[4]), argc > 5 ? (unsigned)std::atoi(argv[5]) : 1u,
+                         argc > 6 ? std::atof(argv[6]) : 0.0, argc > 7 ? std::atoi(argv[7]) : 1);
+    std::fprintf(stderr, "usage: %s case <spec> | bench <nx> <ny> <steps> [seed [max_seconds min_steps]]\n",
+                 argv[0]);
     return 2;
 }

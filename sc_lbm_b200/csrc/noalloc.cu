@@ -2,11 +2,16 @@
 //
 // Some callers cannot allocate device memory: a host application that hands
 // the library a fixed arena and forbids further cudaMalloc (hard memory
-// budgets, custom allocators), or code running where allocation is not
-// allowed, such as between the steps of a captured CUDA graph.  For them this
-// variant of sclbm_domain_mass_momentum works directly on the caller's device
-// buffers and keeps its per-chunk partial sums in a file-scope __device__
-// array instead of memory it allocates.
+// budgets, custom allocators), or a region of a program in which the caller
+// has promised its memory manager that no further device allocation happens.
+// For them this variant of sclbm_domain_mass_momentum works directly on the
+// caller's device buffers and keeps its per-chunk partial sums in a file-scope
+// __device__ array instead of memory it allocates.
+//
+// It returns its result to the host, so it synchronises its stream: it must
+// not be called while that stream is being captured into a CUDA graph, and it
+// refuses a capturing stream (SCLBM_E_INVALID_ARGUMENT) before touching it, so
+// the caller's capture stays intact.
 //
 // The array holds NOALLOC_MAX_PARTIALS partial sums of NOALLOC_CHUNK nodes
 // each, which bounds the lattice to NOALLOC_MAX_PARTIALS * NOALLOC_CHUNK
@@ -15,6 +20,10 @@
 // exits.  Each chunk's slot is overwritten on every call, so nothing needs
 // clearing between calls, but all calls share the one array: calls that
 // overlap on the GPU (different streams, or host threads) race.
+//
+// The first call on a device looks the array's device address up and loads
+// all of this file's kernels (every precision), so later calls on that device
+// make the runtime neither allocate nor load a module.
 #include <mutex>
 
 #include "domain.h"
@@ -115,6 +124,17 @@ int scratch_for_current_device(double **out)
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(scratch)");
+        // with lazy module loading each kernel would otherwise be loaded at its
+        // own first launch, i.e. possibly inside the caller's no-allocation region
+        cudaFuncAttributes fa;
+        const void *kernels[] = {(const void *)k_noalloc_partials<double>,
+                                 (const void *)k_noalloc_partials<float>,
+                                 (const void *)k_noalloc_partials<__half>,
+                                 (const void *)k_noalloc_final};
+        for (const void *k : kernels) {
+            e = cudaFuncGetAttributes(&fa, k);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaFuncGetAttributes(allocation-free monitor)");
+        }
         g_scratch_ptr[dev] = static_cast<double *>(p);
     }
     *out = g_scratch_ptr[dev];
@@ -138,17 +158,31 @@ extern "C" int sclbm_mass_momentum_noalloc(const void *f0, const void *f1, const
     if (ncomp != 1 && ncomp != 2) return set_error(SCLBM_E_INVALID_ARGUMENT, "ncomp must be 1 or 2");
     if (precision < SCLBM_FP64 || precision > SCLBM_FP16_SHIFTED)
         return set_error(SCLBM_E_INVALID_ARGUMENT, "unknown precision");
-    const size_t N = nx * ny;
     if (nx == 0 || ny == 0) return set_error(SCLBM_E_INVALID_ARGUMENT, "empty lattice");
+    // compare before multiplying: nx * ny may wrap around
+    if (ny > (size_t(1) << 27) / nx)
+        return set_error(SCLBM_E_INVALID_ARGUMENT,
+                         "lattice too large for the allocation-free monitor: at most 2^27 nodes "
+                         "(its fixed scratch holds 2048 partial sums of 65536 nodes)");
+    const size_t N = nx * ny;
     const long long nparts = ((long long)N + NOALLOC_CHUNK - 1) / NOALLOC_CHUNK;
     if (nparts > NOALLOC_MAX_PARTIALS)
         return set_error(SCLBM_E_INVALID_ARGUMENT,
                          "lattice too large for the allocation-free monitor: at most 2^27 nodes "
                          "(its fixed scratch holds 2048 partial sums of 65536 nodes)");
+    cudaStream_t s = (cudaStream_t)cuda_stream;
+    // the result is read back with a stream synchronisation, which would
+    // invalidate a capture in progress: refuse before enqueueing anything
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t ce = cudaStreamIsCapturing(s, &cap);
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamIsCapturing");
+    if (cap != cudaStreamCaptureStatusNone)
+        return set_error(SCLBM_E_INVALID_ARGUMENT,
+                         "the allocation-free monitor synchronises its stream and cannot run "
+                         "while the stream is being captured");
     double *scratch = nullptr;
     int rc = scratch_for_current_device(&scratch);
     if (rc) return rc;
-    cudaStream_t s = (cudaStream_t)cuda_stream;
     const int shifted = precision != SCLBM_FP64;
     const double r0 = shifted && rho_ref ? rho_ref[0] : 0.0;
     const double r1 = shifted && rho_ref && ncomp > 1 ? rho_ref[1] : 0.0;

@@ -31,6 +31,8 @@ import tempfile
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# the reference checkout whose unmodified scripts generate the fixtures
+REF_ROOT = os.environ.get("SCLBM_REF", "/root/reference")
 sys.path.insert(0, HERE)
 
 import contact_fields  # noqa: E402
@@ -39,8 +41,8 @@ import cases  # noqa: E402
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from oracle import pyoracle  # noqa: E402
 
-SCRIPT = ("/root/reference/benchmarks/two_phase_two_components_flows/contact_angles/"
-          "compute_contact_angles.py")
+SCRIPT = os.path.join(REF_ROOT, "benchmarks/two_phase_two_components_flows/contact_angles/"
+                      "compute_contact_angles.py")
 
 RUNNER = r"""
 import runpy, sys, types

@@ -24,12 +24,14 @@ import tempfile
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# the reference checkout whose unmodified scripts generate the fixtures
+REF_ROOT = os.environ.get("SCLBM_REF", "/root/reference")
 sys.path.insert(0, HERE)
 
 import laplace_fields  # noqa: E402
 
-SCRIPT = ("/root/reference/benchmarks/two_phase_two_components_flows/laplace_law/"
-          "compute_surface_tension.py")
+SCRIPT = os.path.join(REF_ROOT, "benchmarks/two_phase_two_components_flows/laplace_law/"
+                      "compute_surface_tension.py")
 
 RUNNER = r"""
 import json, runpy, sys, types

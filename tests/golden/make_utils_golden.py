@@ -16,7 +16,9 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-UTILS = "/root/reference/scripts/benchmark_utils.py"
+# the reference checkout whose unmodified scripts generate the fixtures
+REF_ROOT = os.environ.get("SCLBM_REF", "/root/reference")
+UTILS = os.path.join(REF_ROOT, "scripts/benchmark_utils.py")
 
 # (nx, ny, dPdL, direction, mu)
 CHANNELS = [(200, 50, 1e-6, "x", 1.0 / 6.0), (30, 80, 2.5e-5, "y", 0.1)]

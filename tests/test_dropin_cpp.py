@@ -29,7 +29,7 @@ PKG = os.path.join(ROOT, "sc_lbm_b200")
 HOST_INC = os.path.join(PKG, "host", "include")
 RUNNER_SRC = os.path.join(ROOT, "oracle", "ref_runner.cpp")
 STEP_SRC = os.path.join(ROOT, "tests", "cpp", "dropin_step.cpp")
-REF_SRC = "/root/reference"
+REF_SRC = os.environ.get("SCLBM_REF", "/root/reference")
 
 ALL = cases.all_cases()
 MASKS = {k: v for k, v in ALL.items() if v["mode"] == "mask"}

@@ -137,3 +137,28 @@ def test_lattice_beyond_32bit_offsets(sclbm):
     for c in (0, 1):
         assert abs(m1[3 * c] - m0[3 * c]) / m0[3 * c] < 1e-3
     del d
+
+
+@pytest.mark.parametrize("k", [3, 4])
+def test_unstable_ensemble_member_blows_up_with_the_reference(sclbm, k):
+    """Ensemble members that go non-finite do so at the reference's step: the
+    FP64 domain equals the oracle bit for bit one step before (the oracle is
+    pinned to the compiled reference at that step, and the reference is shown
+    to go non-finite at the next one, tests/test_ensemble_blowup_cpu.py), and
+    the monitor reports non-finite populations after the next step."""
+    from oracle import pyoracle
+    from sc_lbm_b200 import capi, workloads as W
+    from test_ensemble_blowup_cpu import BLOWUP, member_case
+    s = BLOWUP[k]
+    case, m = member_case(k, s - 1)
+    want = pyoracle.run_case(case)
+    d = sclbm.Domain(m["nx"], m["ny"], m["mask"], W.params_of(m, sclbm), sclbm.FP64)
+    d.upload_f(0, m["f1"])
+    d.upload_f(1, m["f2"])
+    d.step(s - 1)
+    for comp, key in ((0, "c1_f"), (1, "c2_f")):
+        assert d.download_f(comp).tobytes() == want[key].tobytes(), (k, key)
+    d.mass_momentum()  # all finite
+    d.step(1)
+    with pytest.raises(capi.SclbmNonFinite):
+        d.mass_momentum()

@@ -60,7 +60,7 @@ def test_reference_arm_under_torchrun_two_ranks():
     port = _free_port()
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), "bench.py", "--impl",
-           "reference", "--gpus", "2", "--steps", "1", "--warmup", "3"]
+           "reference", "--gpus", "2", "--steps", "1", "--warmup", "3", "--lattice", "256", "256"]
     r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
@@ -68,3 +68,19 @@ def test_reference_arm_under_torchrun_two_ranks():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["cores"] == 1
+    assert d["config"]["lattice"] == [256, 256] and "reduced" in d["config"]["workload"]
+    assert d["cpu_baseline"]["cpu_model"] and d["cpu_baseline"]["pinned_core"] is not None
+
+
+def test_bench_gpus_two_launches_its_own_ranks():
+    """`bench.py --gpus 2` without torchrun starts both rank processes itself."""
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT")}
+    cmd = [sys.executable, "bench.py", "--impl", "reference", "--gpus", "2", "--steps", "2",
+           "--warmup", "3", "--lattice", "128", "128"]
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["n_gpus"] == 2 and d["config"]["timed_steps"] == 2

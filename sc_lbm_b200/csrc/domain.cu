@@ -280,6 +280,7 @@ static void fill2(const sclbm_domain *d, Fused2Args<S, T> &a)
     a.solid_from_mask = 1;
     a.has_solid = d->has_solid ? 1 : 0;
     a.solids_zero = 1; // creation, uploads and initialisers write 0 at solid nodes
+    a.status = d->d_status;
 }
 
 void domain_fused2_args(const sclbm_domain *d, Fused2Args<double, double> *a64,
@@ -288,6 +289,12 @@ void domain_fused2_args(const sclbm_domain *d, Fused2Args<double, double> *a64,
     if (a64) fill2(d, *a64);
     if (a32) fill2(d, *a32);
     if (a16) fill2(d, *a16);
+}
+
+// rows of the domain start on 16-byte boundaries (the ring kernel's copies)
+static bool ring_row_aligned(const sclbm_domain *d)
+{
+    return d->nx % (16 / elem_size(d->prec)) == 0;
 }
 
 template <typename S, typename T>
@@ -326,6 +333,15 @@ static cudaError_t step_one(const sclbm_domain *d, cudaStream_t s)
     // (FP64 at 4096^2: register tile 17.4 GLUPS all-fluid, 15.4 at 60 % fluid,
     // against 16.4 and 14.8 for the pipelined kernel); 3 and 9 force the
     // pipelined kernel
+    // 11, 12, 13: the ring kernel (bulk row copies into shared memory) with its
+    // default, fewer and more stages; lattices whose rows do not start on
+    // 16-byte boundaries take the register tile
+    if (d->variant >= 11 && d->variant <= 13 && ring_row_aligned(d)) {
+        const int st = d->variant == 11 ? 0 : (d->variant == 12 ? -1 : 1);
+        if constexpr (sizeof(S) == 8) return launch_ring2_fp64(a, st, s);
+        else if constexpr (sizeof(S) == 4) return launch_ring2_f32(a, st, s);
+        else return launch_ring2_f16(a, st, s);
+    }
     const bool pipelined = d->variant == 3 || d->variant == 9;
     if (pipelined) {
         const bool uni = d->variant == 9;
@@ -335,7 +351,7 @@ static cudaError_t step_one(const sclbm_domain *d, cudaStream_t s)
     // variant 1: two pass; 4: register tile with L2 row prefetch; 8: register
     // tile with the uniform solid form; variant 2 (and the FP16 form):
     // register-tile single pass
-    int v = d->variant == 1 || d->variant >= 4 ? d->variant : 0;
+    int v = d->variant == 1 || (d->variant >= 4 && d->variant <= 9) ? d->variant : 0;
     // variant 0 on an FP32/FP16 lattice with solid nodes: the uniform solid
     // form (4096^2 FP32 at 60 % fluid: 29.7 vs 24.0 GLUPS; FP16 36.3 vs 32.7;
     // FP64 runs it slower, 13.9 vs 15.4)
@@ -384,6 +400,7 @@ void sclbm_domain_destroy(sclbm_domain *d)
     if (d->d_mask) cudaFree(d->d_mask);
     if (d->staging) cudaFree(d->staging);
     if (d->partials) cudaFree(d->partials);
+    if (d->d_status) cudaFree(d->d_status);
     delete d;
 }
 
@@ -434,6 +451,11 @@ int sclbm_domain_create(size_t nx, size_t ny, const int32_t *mask, const sclbm_p
     d->partial_blocks = sm_count() * 4;
     if ((rc = dom_alloc(d, (void **)&d->partials, (size_t)(d->partial_blocks + 1) * 8 * sizeof(double))))
         goto fail;
+    if ((rc = dom_alloc(d, (void **)&d->d_status, sizeof(int)))) goto fail;
+    if (cudaMemsetAsync(d->d_status, 0, sizeof(int), s) != cudaSuccess) {
+        rc = set_error(SCLBM_E_CUDA, "memset");
+        goto fail;
+    }
     if (cudaMemcpyAsync(d->d_mask, hm.data(), N, cudaMemcpyHostToDevice, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess) {
         rc = set_error(SCLBM_E_CUDA, "mask upload");
@@ -449,7 +471,8 @@ fail:
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y)
 {
     if (!d) return set_error(SCLBM_E_INVALID_ARGUMENT, "null domain");
-    if (variant < 0 || variant > 9) return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0..9");
+    if (variant < 0 || variant > 13 || variant == 10)
+        return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0..9 or 11..13");
     if (tile_y < 0 || tile_y > 4096) return set_error(SCLBM_E_INVALID_ARGUMENT, "bad tile_y");
     if (variant == 1 && !d->rho_tmp[0] && d->ncomp == 2) {
         const size_t es = d->prec == SCLBM_FP64 ? 8 : 4;
@@ -700,7 +723,12 @@ int sclbm_domain_mass_momentum(sclbm_domain *d, double out[7])
     k_monitor_final<<<1, 256, 0, s>>>(nb, d->partials, res);
     SCLBM_LAUNCHED("monitor final");
     SCLBM_CUDA(cudaMemcpyAsync(out, res, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    int status = 0;
+    SCLBM_CUDA(cudaMemcpyAsync(&status, d->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
     SCLBM_CUDA(cudaStreamSynchronize(s));
+    if (status != 0)
+        return set_error(SCLBM_E_RUNTIME, "a fused-step kernel gave up waiting for its row copies; "
+                                          "the populations are not valid");
     if (out[6] != 0.0) return set_error(SCLBM_E_NONFINITE, "non-finite populations in the domain");
     return SCLBM_OK;
 }

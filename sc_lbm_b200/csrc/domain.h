@@ -13,6 +13,7 @@ struct sclbm_domain {
     void *rho_tmp[2] = {nullptr, nullptr}; // density arrays of the two-pass variant
     double *staging = nullptr;             // N doubles, host<->device conversions
     double *partials = nullptr;            // per-CTA partial sums of the monitor
+    int *d_status = nullptr;               // set by a kernel whose bounded wait ran out
     int partial_blocks = 0;
     int variant = 0;  // 0 single pass, 1 two pass
     int tile_y = 0;   // rows per tile (0: default)

@@ -1,0 +1,289 @@
+// fused_ring.cuh -- the fused two-component step with its population rows
+// streamed into a shared-memory ring by bulk asynchronous copies (the TMA
+// engine: cp.async.bulk global -> shared, completion counted in bytes on an
+// mbarrier per ring stage).
+//
+// Why.  The register-tile kernel (fused_step.cuh) keeps at most one row of
+// loads in flight per warp, and the registers that hold them cap residency;
+// its FP32 and FP16 forms wait on load latency.  Here the bytes in flight do
+// not live in registers: each CTA keeps R - 2 whole population rows on their
+// way into shared memory while its threads reduce and collide the two rows
+// before them.  One copy per population array and row replaces eighteen
+// per-thread loads and their address arithmetic.
+//
+// Work decomposition.  A CTA of RING_W threads owns a strip of RING_W interior
+// columns and a band of rows; the bands split every strip at the same rows
+// and are sized so that every CTA of the grid is resident at once (one wave,
+// no tail).  Neighbouring bands march in opposite directions, so the two
+// halo rows that a pair of bands shares are read by both near the same time
+// and the second read hits L2.
+//
+// Ring.  Row j of a band (j = 0 .. nrow+1, halo rows included) lives in stage
+// j % R: 18 arrays (component k, direction i) of P = RING_W + 2A elements,
+// lattice columns xb - A .. xb + RING_W + A - 1, where A elements make 16 bytes
+// (copies start and end on 16-byte boundaries: nx must be a multiple of A).
+// Iteration j waits for row j, reduces it to both components' densities
+// (density ring in shared memory, one __syncthreads), collides row j - 1 from
+// its populations still in the ring and pushes the results straight to global
+// memory (the scattered push of collide_push, half-way bounce-back included),
+// and then refills the stage of row j - 2, which every thread finished with
+// before the barrier, with row j + R - 2.  The arithmetic per node is the
+// register tile's (collide_push), so both kernels write the same bytes.
+//
+// Waits are bounded: a stage that does not fill within RING_WAIT_LIMIT polls
+// sets *a.status and the CTA skips the rest of its band (no hang); the
+// domain's monitor reports the flag.
+#pragma once
+#include "fused_step.cuh"
+
+namespace sclbm {
+
+constexpr int RING_W = 128;              // interior columns per strip = threads per CTA
+constexpr int RING_WAIT_LIMIT = 1 << 20; // polls of one stage before giving up (~1 s)
+
+// elements per 16 bytes of storage type S
+template <typename S> constexpr int ring_pad() { return 16 / (int)sizeof(S); }
+
+template <typename S, typename T, int R> struct RingLayout {
+    static constexpr int A = ring_pad<S>();
+    static constexpr int P = RING_W + 2 * A;                    // elements per array row
+    static constexpr int Q = RING_W + 2;                        // density ring columns
+    static constexpr size_t stage = size_t(18) * P * sizeof(S); // multiple of 16
+    static constexpr size_t pops = size_t(R) * stage;
+    static constexpr size_t rho = size_t(4) * Q * sizeof(V2<T>);
+    static constexpr size_t msk = size_t(4) * Q;
+    static constexpr size_t bars = (pops + rho + msk + 15) & ~size_t(15);
+    static constexpr size_t bytes = bars + size_t(R) * 8 + 16;
+    static_assert(stage % 16 == 0, "ring stages must keep 16-byte alignment");
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// one arrival that also announces the bytes the stage's copies will deliver
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(bar), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+// bulk copy of `bytes` (multiple of 16) from global src to shared dst (both
+// 16-byte aligned), completing on mbarrier `bar`; no multicast
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+        "l"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+
+// One band of one strip per CTA; band b covers rows [b*ny/bands, (b+1)*ny/bands).
+template <typename S, typename T, int FLAGS, int R, bool WIDE>
+__global__ void __launch_bounds__(RING_W, 1) k_ring2(const __grid_constant__ Fused2Args<S, T> a, int bands)
+{
+    using L = RingLayout<S, T, R>;
+    constexpr int A = L::A, P = L::P, Q = L::Q;
+    constexpr bool SOLID = (FLAGS & KF_SOLID) != 0;
+    extern __shared__ __align__(128) unsigned char ring_smem[];
+    S *pops = reinterpret_cast<S *>(ring_smem);
+    V2<T> *rho = reinterpret_cast<V2<T> *>(ring_smem + L::pops);
+    uint8_t *msk = ring_smem + L::pops + L::rho;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(ring_smem + L::bars);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(ring_smem + L::bars + R * 8);
+
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int nx = a.nx, ny = a.ny;
+    const int xb = blockIdx.x * RING_W;
+    const int ncol = min(RING_W, nx - xb);
+    const int band = blockIdx.y;
+    const int y0 = (int)((long long)band * ny / bands);
+    const int nrow = (int)((long long)(band + 1) * ny / bands) - y0;
+    const bool down = (band & 1) != 0;
+    const bool act = t < ncol;
+    const bool hl = t == 0, hr = t == ncol - 1;
+    const int x = act ? xb + t : xb;
+    const int xl = wrap1(x - 1, nx), xr = wrap1(x + 1, nx);
+    const int xhl = wrap1(xb - 1, nx), xhr = wrap1(xb + ncol, nx);
+    const int last = nrow + 1;
+    // lattice row of ring row j (tile row -1 .. nrow in march order)
+    auto gy = [&](int j) { return wrap1(y0 + (down ? nrow - j : j - 1), ny); };
+
+    if (t == 0) {
+        for (int s = 0; s < R; ++s) mbar_init(smem_addr(&bars[s]), 1);
+        *abort_flag = 0;
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    // warp 0 requests row j: lanes 0..17 copy one population array each
+    const uint32_t row_bytes = 18u * (uint32_t)(ncol + 2 * A) * (uint32_t)sizeof(S);
+    const bool one_copy = xb >= A && xb + ncol + A <= nx;
+    const int left_src = xb >= A ? xb - A : nx - A;        // A columns left of the strip
+    const int right_src = xb + ncol == nx ? 0 : xb + ncol; // A columns right of it
+    auto issue = [&](int j) {
+        const int st = j % R;
+        const uint32_t bar = smem_addr(&bars[st]);
+        if (lane == 0) mbar_expect_tx(bar, row_bytes);
+        __syncwarp();
+        if (lane < 18) {
+            const int k = lane >= 9 ? 1 : 0, i = lane - 9 * k;
+            const S *row = a.fin[k] + (size_t)i * a.N + (size_t)gy(j) * (size_t)nx;
+            S *dst = pops + ((size_t)st * 18 + lane) * P;
+            if (one_copy) {
+                bulk_g2s(smem_addr(dst), row + (xb - A), (uint32_t)((ncol + 2 * A) * sizeof(S)), bar);
+            } else {
+                bulk_g2s(smem_addr(dst), row + left_src, (uint32_t)(A * sizeof(S)), bar);
+                bulk_g2s(smem_addr(dst + A), row + xb, (uint32_t)(ncol * sizeof(S)), bar);
+                bulk_g2s(smem_addr(dst + A + ncol), row + right_src, (uint32_t)(A * sizeof(S)), bar);
+            }
+        }
+    };
+    auto wait_row = [&](int j) {
+        const uint32_t bar = smem_addr(&bars[j % R]);
+        const uint32_t par = (uint32_t)((j / R) & 1);
+        for (int it = 0; it < RING_WAIT_LIMIT; ++it)
+            if (mbar_try_wait(bar, par)) return true;
+        return false;
+    };
+
+    int issued = -1; // last row requested (warp 0's view)
+    if (warp == 0)
+        for (int j = 0; j < R && j <= last; ++j) {
+            issue(j);
+            issued = j;
+        }
+
+    // masks of the next row, loaded one row ahead
+    uint8_t mn = 1, mnl = 1, mnr = 1;
+    if (SOLID && act) {
+        const size_t row = (size_t)gy(0) * (size_t)nx;
+        mn = a.mask[row + x];
+        if (hl) mnl = a.mask[row + xhl];
+        if (hr) mnr = a.mask[row + xhr];
+    }
+    bool aborted = false;
+    int consumed = -1;
+    for (int j = 0; j <= last; ++j) {
+        const uint8_t m = mn, ml = mnl, mr = mnr;
+        if (SOLID && act && j < last) {
+            const size_t row = (size_t)gy(j + 1) * (size_t)nx;
+            mn = a.mask[row + x];
+            if (hl) mnl = a.mask[row + xhl];
+            if (hr) mnr = a.mask[row + xhr];
+        }
+        const int slot = j & 3;
+        if (!aborted) {
+            if (wait_row(j)) {
+                consumed = j;
+                const S *stg = pops + (size_t)(j % R) * 18 * P;
+                auto density = [&](int col, uint8_t mm, int q) {
+                    T r[2];
+#pragma unroll
+                    for (int k = 0; k < 2; ++k) {
+                        T s = T(0); // 0.0 + f0 + ... + f8, src/fluid.cpp:177-181
+#pragma unroll
+                        for (int i = 0; i < 9; ++i) s += T(stg[(k * 9 + i) * P + col]);
+                        r[k] = s;
+                    }
+                    if (SOLID && !mm) r[0] = r[1] = T(0);
+                    rho[slot * Q + q] = Vec2<T>::make(r[0], r[1]);
+                    msk[slot * Q + q] = SOLID ? mm : 1;
+                };
+                if (act) {
+                    density(A + t, m, t + 1);
+                    if (hl) density(A - 1, ml, 0);
+                    if (hr) density(A + ncol, mr, ncol + 1);
+                }
+            } else {
+                *abort_flag = 1;
+                if (a.status) atomicExch(a.status, 1);
+            }
+        }
+        __syncthreads();
+        aborted = *abort_flag != 0;
+        if (aborted) continue;
+        if (act && j >= 2) {
+            // rows below (sb), at (sc) and above (sa) the node of ring row j-1
+            const int s_old = (j - 2) & 3, sc = (j - 1) & 3, s_new = slot;
+            const int sb = down ? s_new : s_old, sa = down ? s_old : s_new;
+            const int yc = gy(j - 1);
+            const Stencil<T> st{{rho + sb * Q, rho + sc * Q, rho + sa * Q},
+                                {msk + sb * Q, msk + sc * Q, msk + sa * Q}, t + 1};
+            const Nbr n = make_nbr(nx, x, xl, xr, yc, wrap1(yc - 1, ny), wrap1(yc + 1, ny));
+            const RingPops<S, T, P> f{pops + (size_t)((j - 1) % R) * 18 * P + A + t};
+            collide_push<S, T, FLAGS, WIDE>(a, f, st, n);
+        }
+        // the stage of row j-2 was last read before this iteration's barrier
+        if (warp == 0 && j >= 2 && j + R - 2 <= last) {
+            issue(j + R - 2);
+            issued = j + R - 2;
+        }
+    }
+    if (aborted && warp == 0 && lane == 0) {
+        // let the copies still in flight land before the CTA's shared memory is released
+        for (int j = consumed + 1; j <= issued; ++j) (void)wait_row(j);
+    }
+}
+
+template <typename S, typename T, int FLAGS, int R, bool WIDE>
+inline cudaError_t launch_ring2_f(const Fused2Args<S, T> &a, cudaStream_t s)
+{
+    using L = RingLayout<S, T, R>;
+    auto kern = k_ring2<S, T, FLAGS, R, WIDE>;
+    static int per_sm = 0; // resident CTAs per SM of this instantiation (one device)
+    if (per_sm == 0) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes);
+        if (e != cudaSuccess) return e;
+        int n = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, RING_W, L::bytes);
+        if (e != cudaSuccess) return e;
+        if (n < 1) return cudaErrorInvalidConfiguration;
+        per_sm = n;
+    }
+    const int strips = (a.nx + RING_W - 1) / RING_W;
+    const int resident = per_sm * sm_count();
+    // one wave: as many bands as resident CTAs allow, at least 4 rows each
+    int bands = std::max(1, resident / strips);
+    bands = std::min(bands, std::max(1, a.ny / 4));
+    kern<<<dim3(strips, bands), RING_W, L::bytes, s>>>(a, bands);
+    return cudaGetLastError();
+}
+
+// the ring needs rows that start on 16-byte boundaries: nx a multiple of
+// 16 / sizeof(S) (buffers from cudaMalloc are 256-byte aligned)
+template <typename S> inline bool ring_fits(int nx) { return nx % ring_pad<S>() == 0; }
+
+// UNI: lattices with solid nodes run the uniform solid form (KF_UNIFORM)
+template <typename S, typename T, int R, int UNI = KF_UNIFORM>
+inline cudaError_t launch_ring2_any(const Fused2Args<S, T> &a, cudaStream_t s)
+{
+    if (!ring_fits<S>(a.nx) || a.nx < 1 || a.ny < 1) return cudaErrorInvalidValue;
+    if (needs_wide_offsets(a.N)) return launch_ring2_f<S, T, KF_FORCE | KF_SOLID | UNI, R, true>(a, s);
+    switch (kernel_flags(a)) {
+    case 0: return launch_ring2_f<S, T, 0, R, false>(a, s);
+    case KF_FORCE: return launch_ring2_f<S, T, KF_FORCE, R, false>(a, s);
+    case KF_SOLID: return launch_ring2_f<S, T, KF_SOLID | UNI, R, false>(a, s);
+    default: return launch_ring2_f<S, T, KF_FORCE | KF_SOLID | UNI, R, false>(a, s);
+    }
+}
+
+} // namespace sclbm

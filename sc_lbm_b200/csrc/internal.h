@@ -94,6 +94,8 @@ template <typename S, typename T> struct Fused2Args {
     int has_solid;                       // the mask has solid nodes (else all fluid)
     int solids_zero;                     // both buffers hold 0 at solid nodes: the kernels
                                          // neither read nor write them (domain path)
+    int *status;                         // set to 1 by a kernel whose bounded wait ran out
+                                         // (ring kernel), or null
 };
 
 // arguments of the single-component fused kernel
@@ -128,6 +130,13 @@ cudaError_t launch_batch2_async_fp64(const Fused2Args<double, double> *doms, con
                                      int ntiles, int grid, int parity, cudaStream_t s);
 cudaError_t launch_batch2_async_f32(const Fused2Args<float, float> *doms, const BandTile *tiles,
                                     int ntiles, int grid, int parity, cudaStream_t s);
+// ring kernels (fused_ring.cuh): population rows streamed into shared memory
+// by bulk asynchronous copies; stages selects the ring depth (0 default, -1
+// fewer, +1 more); cudaErrorInvalidValue when nx is not a multiple of
+// 16 / sizeof(storage)
+cudaError_t launch_ring2_fp64(const Fused2Args<double, double> &a, int stages, cudaStream_t s);
+cudaError_t launch_ring2_f32(const Fused2Args<float, float> &a, int stages, cudaStream_t s);
+cudaError_t launch_ring2_f16(const Fused2Args<__half, float> &a, int stages, cudaStream_t s);
 int async_resident_fp64(); // CTAs of the batched kernel resident on the device
 int async_resident_f32();
 constexpr int ASYNC_STRIP = 128;

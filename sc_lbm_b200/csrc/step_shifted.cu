@@ -98,6 +98,24 @@ int batch_blocks_per_sm(sclbm_precision p, int body)
 }
 } // namespace sclbm
 
+#include "fused_ring.cuh"
+namespace sclbm {
+// FP32: 9.8 KB per stage, five stages (three rows in flight) keep four CTAs
+// per SM; FP16: 5.2 KB per stage, eight stages
+cudaError_t launch_ring2_f32(const Fused2Args<float, float> &a, int stages, cudaStream_t s)
+{
+    if (stages < 0) return launch_ring2_any<float, float, 4>(a, s);
+    if (stages > 0) return launch_ring2_any<float, float, 6>(a, s);
+    return launch_ring2_any<float, float, 5>(a, s);
+}
+cudaError_t launch_ring2_f16(const Fused2Args<__half, float> &a, int stages, cudaStream_t s)
+{
+    if (stages < 0) return launch_ring2_any<__half, float, 6>(a, s);
+    if (stages > 0) return launch_ring2_any<__half, float, 10>(a, s);
+    return launch_ring2_any<__half, float, 8>(a, s);
+}
+} // namespace sclbm
+
 #include "fused_async.cuh"
 namespace sclbm {
 cudaError_t launch_fused2_async_f32(const Fused2Args<float, float> &a, cudaStream_t s, bool uniform)

@@ -72,14 +72,17 @@ def test_domain_fp64_bit_exact(sclbm, name):
                                                (64, 64, 1), (128, 0, 0), (128, 0, 3), (128, 0, 4),
                                                (128, 3, 4), (128, 0, 5), (128, 4, 5),
                                                (128, 0, 7), (128, 0, 8), (128, 3, 8),
-                                               (128, 0, 9), (32, 0, 2), (32, 5, 8), (32, 4, 1)])
+                                               (128, 0, 9), (32, 0, 2), (32, 5, 8), (32, 4, 1),
+                                               (128, 0, 11), (128, 0, 12), (128, 0, 13)])
 def test_domain_fp64_tiling_invariant(sclbm, tx, tile_y, variant):
     """Kernel variant (pipelined persistent, two pass, register tile, register
-    tile with L2 prefetch) and tile shape do not change a single bit."""
+    tile with L2 prefetch, ring of bulk row copies at three depths) and tile
+    shape do not change a single bit."""
     for name in ("porous_96x48", "spinodal_48x40", "channel_80x32", "droplet_solid_flow"):
         res = gpu_runner.run_domain(sclbm, RUNS[name], sclbm.FP64, variant=variant,
                                     tile_y=tile_y, tx=tx)
         assert_golden(name, res, [k for k in res if k.endswith(("_f", "_final"))])
+        res["_domain"].mass_momentum()  # raises if a bounded wait ran out
 
 
 def test_tiny_and_ragged_lattices(sclbm, oracle):
@@ -150,7 +153,8 @@ def test_shifted_forms_density_error(sclbm, oracle, name, steps, prec, tol_max, 
                                                (5, 0, 128), (5, 7, 128), (5, 1, 128), (5, 2, 128),
                                                (6, 0, 128), (6, 1, 128), (6, 5, 128), (6, 64, 128),
                                                (7, 0, 128), (7, 3, 128), (8, 0, 128), (8, 5, 128),
-                                               (9, 0, 128), (0, 0, 32), (2, 3, 32), (8, 7, 32)])
+                                               (9, 0, 128), (0, 0, 32), (2, 3, 32), (8, 7, 32),
+                                               (11, 0, 128), (12, 0, 128), (13, 0, 128)])
 def test_shifted_variants_match_register_tile(sclbm, variant, tile_y, tx):
     """The shifted forms give the same bytes with every kernel variant and
     tile width."""
@@ -162,6 +166,37 @@ def test_shifted_variants_match_register_tile(sclbm, variant, tile_y, tx):
                                   variant=variant, tile_y=tile_y, tx=tx)
         assert a["c1_f"].tobytes() == b["c1_f"].tobytes()
         assert a["c2_f"].tobytes() == b["c2_f"].tobytes()
+        b["_domain"].mass_momentum()
+
+
+# lattices for the ring kernel: partial last strips, strips narrower than the
+# 16-byte copy window, single rows, and widths whose rows are not 16-byte
+# aligned in some storage forms (those domains take the register tile)
+RING_LATTICES = [(8, 3, []), (136, 20, [("walls", 1, "x")]), (264, 9, [("circle", 5, 130, 4)]),
+                 (16, 1, []), (4, 7, [("walls", 1, "y")]), (130, 6, [("walls", 1, "x")]),
+                 (256, 33, [("circle", 9, 200, 16), ("walls", 1, "x")])]
+
+
+@pytest.mark.parametrize("nx,ny,geom", RING_LATTICES)
+def test_ring_kernel_ragged_lattices(sclbm, oracle, nx, ny, geom):
+    """Ring kernel (variant 11) on awkward shapes: FP64 bit for bit with the
+    oracle, FP32/FP16 byte for byte with the register tile."""
+    f = np.concatenate([cases.noisy_f_equilibrium(nx + 3 * ny, nx, ny, 1.0, 0.02, 0.03),
+                        cases.noisy_f_equilibrium(nx + 5 * ny, nx, ny, 0.4, 0.02, 0.03)])
+    case = dict(nx=nx, ny=ny, geom=geom, mode="two", fluid1=(0.9, 1.1, 0.1),
+                fluid2=(1.2, 1.1, -0.1), init=("file", f),
+                force=(3, cases.force_vec(1e-4, "x")), steps=9)
+    want = oracle.run_case(case)
+    got = gpu_runner.run_domain(sclbm, case, sclbm.FP64, variant=11)
+    for k in ("c1_f", "c2_f", "c1_rho_final", "c2_ux_final"):
+        assert got[k].tobytes() == want[k].tobytes(), (nx, ny, k)
+    got["_domain"].mass_momentum()
+    for prec in (sclbm.FP32_SHIFTED, sclbm.FP16_SHIFTED):
+        a = gpu_runner.run_domain(sclbm, case, prec, rho_ref=(1.0, 0.4))
+        b = gpu_runner.run_domain(sclbm, case, prec, rho_ref=(1.0, 0.4), variant=11)
+        assert a["c1_f"].tobytes() == b["c1_f"].tobytes(), (nx, ny, prec)
+        assert a["c2_f"].tobytes() == b["c2_f"].tobytes(), (nx, ny, prec)
+        b["_domain"].mass_momentum()
 
 
 # ------------------------------------------------------------------- monitors

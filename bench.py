@@ -239,6 +239,71 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def cpu_config_runs(sample_steps=10, members=8, member_steps=200):
+    """The reference's serial code on every configuration, pinned to one core:
+    full runs of the Poiseuille channel (200x50, 10,000 steps) and the Laplace
+    droplet (256x256, radius 40, 20,000 steps); `sample_steps` steady steps of
+    the 2048x1024 drainage lattice; `member_steps` steps of each of the first
+    `members` ensemble domains (the ensemble's serial time is estimated from
+    their aggregate rate); and the 4096x4096 two-component lattice, the
+    stand-in for the 16384x8192 spinodal lattice (about 80 GB of host memory
+    in the reference's layout), whose per-node work it shares."""
+    from oracle import pyoracle
+    from sc_lbm_b200 import workloads as W
+    info = pyoracle.cpu_info()
+    core = info["pin_core"]
+
+    def two(w, steps, fl1, fl2, force=(0, [0.0] * 9)):
+        nx, ny = w["nx"], w["ny"]
+        m = np.asarray(w["mask"]).reshape(ny, nx)
+        ys, xs = np.nonzero(m == 0)
+        return dict(nx=nx, ny=ny, geom=[("solid_node", int(x), int(y)) for y, x in zip(ys, xs)],
+                    mode="two", fluid1=fl1, fluid2=fl2,
+                    init=("file", np.concatenate([w["f1"], w["f2"]])), force=force, steps=steps)
+
+    def timed(label, case, full):
+        r = pyoracle.run_ref(case, core=core, timing=True)
+        t = float(r["loop_seconds"][0])
+        n = case["nx"] * case["ny"]
+        return {"config": label, "lattice": [case["nx"], case["ny"]], "steps": case["steps"],
+                "full_run": full, "loop_seconds": round(t, 3),
+                "mlups": round(n * case["steps"] / t / 1e6, 4)}
+
+    out = []
+    w = W.poiseuille()
+    out.append(timed("1 poiseuille 200x50 FP64", dict(
+        nx=200, ny=50, geom=[("walls", 1, "x")], mode="single", fluid1=(1.0, 0, 0),
+        init=("simple", 1.0), force=(1, list(w["force"])), steps=10000), True))
+    w = W.laplace(40)
+    out.append(timed("2 laplace 256x256 radius 40", two(w, 20000, (1.0, 0.9, 0.0), (1.0, 0.9, 0.0)),
+                     True))
+    w = W.drainage()
+    out.append(timed("3 drainage 2048x1024 porous (sampled steps)",
+                     two(w, sample_steps, (1.0, 0.9, -0.2), (1.0, 0.9, 0.2),
+                         (1, list(w["force1"]))), False))
+    nodes = t = 0.0
+    sizes = []
+    for k in range(members):
+        m = W.ensemble_member(k)
+        r = timed(f"member {k}", two(m, member_steps, (m["tau"][0], m["G"], m["Gs"][0]),
+                                     (m["tau"][1], m["G"], m["Gs"][1])), False)
+        nodes += m["nx"] * m["ny"] * member_steps
+        t += r["loop_seconds"]
+        sizes.append([m["nx"], m["ny"]])
+    ens = W.ensemble(512)
+    total = sum(m["nx"] * m["ny"] for m in ens)
+    out.append({"config": "4 ensemble of 512 (sampled members, serial)", "members_timed": sizes,
+                "steps": member_steps, "full_run": False, "mlups": round(nodes / t / 1e6, 4),
+                "estimated_serial_seconds_10000_steps": round(total * 10000 / (nodes / t), 1)})
+    r = pyoracle.ref_bench(4096, 4096, 4, core=core, max_seconds=120.0, min_steps=2)
+    per = r["step_seconds"][1:]
+    out.append({"config": "5 spinodal (4096x4096 stand-in for 16384x8192, sampled steps)",
+                "lattice": [4096, 4096], "steps": len(per), "full_run": False,
+                "mlups": round(4096 * 4096 * len(per) / sum(per) / 1e6, 4)})
+    return {"cores": 1, "pinned_core": core, "cpu_model": info["model"], "nproc": info["nproc"],
+            "kind": "reference", "runs": out}
+
+
 def cpu_port_steps(nx, ny, steps, core=None, budget_s=0.0, min_steps=1):
     """Per-step seconds of the C restatement (oracle/) -- the fallback CPU arm
     (this process pinned to `core` while it runs)."""
@@ -282,48 +347,36 @@ def cpu_port_steps(nx, ny, steps, core=None, budget_s=0.0, min_steps=1):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def density_errors(a, b):
-    """max |a-b| / mean |b| and ||a-b||_2 / ||b||_2 (density scale of the component)."""
-    d = a - b
-    return float(np.max(np.abs(d)) / np.mean(np.abs(b))), float(np.linalg.norm(d) / np.linalg.norm(b))
-
-
 def accuracy_report(sc, mask, params, f1, f2, checkpoints=(20, 200)):
     """Shifted forms against the FP64 GPU form (itself bit-exact with the
     reference) from the same start, plus an FP64 twin whose component-1
     populations start one ulp away: the twin's divergence is the amplification
-    the spinodal dynamics applies to any rounding difference."""
+    the spinodal dynamics applies to any rounding difference.  Per component:
+    density error max and RMS over the mean density, velocity (u = j / rho)
+    error max over max |u| and RMS over RMS |u|; mass drift per component."""
+    from sc_lbm_b200.validation import compare_domains, mass_drift, twin_populations
     NXY = mask.size
     doms = {"fp64": sc.Domain(NX, NY, mask, params, sc.FP64),
             "fp64_1ulp_twin": sc.Domain(NX, NY, mask, params, sc.FP64),
             "fp32s": sc.Domain(NX, NY, mask, params, sc.FP32_SHIFTED),
             "fp16s": sc.Domain(NX, NY, mask, params, sc.FP16_SHIFTED)}
     for name, d in doms.items():
-        d.upload_f(0, np.nextafter(f1, np.inf) if name == "fp64_1ulp_twin" else f1)
+        d.upload_f(0, twin_populations(f1) if name == "fp64_1ulp_twin" else f1)
         d.upload_f(1, f2)
     m0 = {k: d.mass_momentum() for k, d in doms.items()}
-    rep, done = {"metric": "max|drho|/mean(rho), L2 |drho|/|rho| per component vs FP64"}, 0
+    rep, done = {"metric": "per component: rho_max / rho_rms = max / RMS |drho| over mean rho; "
+                           "u_max = max |du| / max |u|, u_rms = RMS |du| / RMS |u|; vs FP64"}, 0
     for cp in checkpoints:
         for d in doms.values():
             d.step(cp - done)
         done = cp
-        ref = [doms["fp64"].download_rho(k) for k in range(2)]
-        row = {}
-        for name in ("fp32s", "fp16s", "fp64_1ulp_twin"):
-            errs = [density_errors(doms[name].download_rho(k), ref[k]) for k in range(2)]
-            row[name] = {"max_over_mean": [e[0] for e in errs], "l2": [e[1] for e in errs]}
-        ux, _ = doms["fp32s"].download_velocity(0)
-        u64, _ = doms["fp64"].download_velocity(0)
-        row["fp32s"]["ux_max_err_over_max_u"] = float(np.max(np.abs(ux - u64)) / np.max(np.abs(u64)))
-        rep[f"step_{cp}"] = row
-    drift = {}
-    for name, d in doms.items():
-        m1 = d.mass_momentum()
-        drift[name] = [float((m1[3 * k] - m0[name][3 * k]) / m0[name][3 * k]) for k in range(2)]
-    rep["mass_drift"] = drift
+        rep[f"step_{cp}"] = compare_domains(doms)
+    rep["mass_drift"] = {k: mass_drift(d, m0[k]) for k, d in doms.items()}
     rep["nodes"] = NXY
     del doms
     return rep
+
+
 def time_domain(torch, sc, dom, stream, steps, warmup):
     """Device time of `steps` fused steps, CUDA events on the launching stream."""
     dom.step(warmup)
@@ -544,13 +597,22 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-domain ensemble leg")
+    ap.add_argument("--cpu-configs", action="store_true",
+                    help="time the reference's serial code on every configuration (CPU only)")
+    ap.add_argument("--out", default=None, help="--cpu-configs: write the results here")
     ap.add_argument("--lattice", type=int, nargs=2, default=[NX, NY], metavar=("NX", "NY"),
                     help="reference arm only: a smaller lattice for quick checks (labelled)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         sys.exit(self_launch(sys.argv[1:], args.gpus))
-    if args.impl == "reference":
+    if args.cpu_configs:
+        res = cpu_config_runs()
+        print(json.dumps(res), flush=True)
+        if args.out:
+            with open(args.out, "w") as fh:
+                json.dump(res, fh, indent=1)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

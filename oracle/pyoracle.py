@@ -315,10 +315,12 @@ def read_ref_output(path: str) -> dict:
     return out
 
 
-def run_ref(case, runner: str | None = None) -> dict:
+def run_ref(case, runner: str | None = None, core=None, timing: bool = False) -> dict:
     """Run a case through the compiled reference (oracle/_ref), or through
     ``runner``: the same driver source (ref_runner.cpp) built against another
-    implementation of the reference's Geometry / Fluid / LBM classes."""
+    implementation of the reference's Geometry / Fluid / LBM classes.  `core`
+    pins the run to one CPU; with `timing`, ``loop_seconds`` (the main loop's
+    time) is returned with the arrays."""
     if runner is None:
         if not have_ref():
             raise FileNotFoundError("oracle/_ref/sclbm_ref_runner was not built")
@@ -331,8 +333,12 @@ def run_ref(case, runner: str | None = None) -> dict:
             np.asarray(case["init"][1], dtype="<f8").tofile(init_path)
         with open(spec, "w") as fh:
             fh.write(_spec_text(case, init_path, out_path))
-        subprocess.run([runner, "case", spec], check=True, stdout=subprocess.DEVNULL)
-        return read_ref_output(out_path)
+        cmd, pre = _pinned([runner, "case", spec], core)
+        subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, preexec_fn=pre)
+        res = read_ref_output(out_path)
+        if not timing:
+            res.pop("loop_seconds", None)
+        return res
 
 
 def ref_bench_parallel(nx: int, ny: int, steps: int, instances: int) -> dict:
@@ -369,7 +375,7 @@ def cpu_info() -> dict:
         pass
     usable = sorted(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else \
         list(range(os.cpu_count() or 1))
-    return {"model": model, "nproc": os.cpu_count(), "usable": len(usable), "pin_core": usable[0]}
+    return {"model": model, "nproc": os.cpu_count(), "usable": len(usable), "pin_core": usable[-1]}
 
 
 def _pinned(cmd, core):

@@ -259,7 +259,11 @@ template <typename T> static void fill_comp(CompParams<T> &c, const sclbm_params
     c.gs_neg = (T)(-1.0 * p.g_solid[k]);
     c.rho_ref = (T)p.rho_ref[k];
     c.force_on = p.force_on[k];
-    for (int i = 0; i < 9; ++i) c.force[i] = (T)(p.force_on[k] ? p.force[k][i] : 0.0);
+    c.force_sum = (T)0;
+    for (int i = 0; i < 9; ++i) {
+        c.force[i] = (T)(p.force_on[k] ? p.force[k][i] : 0.0);
+        c.force_sum += c.force[i];
+    }
 }
 
 template <typename S, typename T>

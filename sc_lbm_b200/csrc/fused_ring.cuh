@@ -6,9 +6,9 @@
 // Why.  The register-tile kernel (fused_step.cuh) keeps at most one row of
 // loads in flight per warp, and the registers that hold them cap residency;
 // its FP32 and FP16 forms wait on load latency.  Here the bytes in flight do
-// not live in registers: each CTA keeps R - 2 whole population rows on their
-// way into shared memory while its threads reduce and collide the two rows
-// before them.  One copy per population array and row replaces eighteen
+// not live in registers: each CTA keeps R whole population rows on their way
+// into shared memory while its threads reduce one row and collide the one
+// before it.  One copy per population array and row replaces eighteen
 // per-thread loads and their address arithmetic.
 //
 // Work decomposition.  A CTA of RING_W threads owns a strip of RING_W interior
@@ -18,17 +18,18 @@
 // halo rows that a pair of bands shares are read by both near the same time
 // and the second read hits L2.
 //
-// Ring.  Row j of a band (j = 0 .. nrow+1, halo rows included) lives in stage
+// Ring.  Row j of a band (j = 0 .. nrow+1, halo rows included) lands in stage
 // j % R: 18 arrays (component k, direction i) of P = RING_W + 2A elements,
 // lattice columns xb - A .. xb + RING_W + A - 1, where A elements make 16 bytes
 // (copies start and end on 16-byte boundaries: nx must be a multiple of A).
-// Iteration j waits for row j, reduces it to both components' densities
-// (density ring in shared memory, one __syncthreads), collides row j - 1 from
-// its populations still in the ring and pushes the results straight to global
-// memory (the scattered push of collide_push, half-way bounce-back included),
-// and then refills the stage of row j - 2, which every thread finished with
-// before the barrier, with row j + R - 2.  The arithmetic per node is the
-// register tile's (collide_push), so both kernels write the same bytes.
+// Iteration j waits for row j, reads each thread's column into registers and
+// reduces it to both components' densities (density ring in shared memory,
+// one __syncthreads); the stage is then free and is refilled at once with row
+// j + R, so all R stages are in flight while the CTA computes; finally row
+// j - 1 is collided from registers and pushed straight to global memory (the
+// scattered push of collide_push, half-way bounce-back included).  The
+// arithmetic per node is the register tile's (collide_push), so both kernels
+// write the same bytes.
 //
 // Waits are bounded: a stage that does not fill within RING_WAIT_LIMIT polls
 // sets *a.status and the CTA skips the rest of its band (no hang); the
@@ -96,9 +97,19 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t
         : "memory");
 }
 
+// resident CTAs per SM the register cap aims at (the ring's shared memory
+// allows at least as many): the register tile's figures, six for FP32
+// arithmetic (five in the uniform solid form, which spills at 80 registers),
+// three for FP64
+template <typename T, int FLAGS> constexpr int ring_min_ctas()
+{
+    return sizeof(T) == 8 ? 3 : ((FLAGS & KF_UNIFORM) ? 5 : 6);
+}
+
 // One band of one strip per CTA; band b covers rows [b*ny/bands, (b+1)*ny/bands).
 template <typename S, typename T, int FLAGS, int R, bool WIDE>
-__global__ void __launch_bounds__(RING_W, 1) k_ring2(const __grid_constant__ Fused2Args<S, T> a, int bands)
+__global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS>()))
+    k_ring2(const __grid_constant__ Fused2Args<S, T> a, int bands)
 {
     using L = RingLayout<S, T, R>;
     constexpr int A = L::A, P = L::P, Q = L::Q;
@@ -182,7 +193,11 @@ __global__ void __launch_bounds__(RING_W, 1) k_ring2(const __grid_constant__ Fus
     }
     bool aborted = false;
     int consumed = -1;
-    for (int j = 0; j <= last; ++j) {
+
+    // iteration j: row j from its stage into registers (cur) and its densities
+    // into the ring; barrier; the stage is free, so request row j + R into it;
+    // collide row j - 1 (prev) from the stencil rows j - 2, j - 1, j
+    auto step_row = [&](const int j, T(&cur)[2][9], const T(&prev)[2][9]) {
         const uint8_t m = mn, ml = mnl, mr = mnr;
         if (SOLID && act && j < last) {
             const size_t row = (size_t)gy(j + 1) * (size_t)nx;
@@ -195,23 +210,39 @@ __global__ void __launch_bounds__(RING_W, 1) k_ring2(const __grid_constant__ Fus
             if (wait_row(j)) {
                 consumed = j;
                 const S *stg = pops + (size_t)(j % R) * 18 * P;
-                auto density = [&](int col, uint8_t mm, int q) {
+                auto density = [&](const T(&f)[2][9], uint8_t mm, int q) {
                     T r[2];
 #pragma unroll
                     for (int k = 0; k < 2; ++k) {
                         T s = T(0); // 0.0 + f0 + ... + f8, src/fluid.cpp:177-181
 #pragma unroll
-                        for (int i = 0; i < 9; ++i) s += T(stg[(k * 9 + i) * P + col]);
+                        for (int i = 0; i < 9; ++i) s += f[k][i];
                         r[k] = s;
                     }
                     if (SOLID && !mm) r[0] = r[1] = T(0);
                     rho[slot * Q + q] = Vec2<T>::make(r[0], r[1]);
                     msk[slot * Q + q] = SOLID ? mm : 1;
                 };
+                auto load = [&](int col, T(&f)[2][9]) {
+#pragma unroll
+                    for (int k = 0; k < 2; ++k)
+#pragma unroll
+                        for (int i = 0; i < 9; ++i) f[k][i] = T(stg[(k * 9 + i) * P + col]);
+                };
                 if (act) {
-                    density(A + t, m, t + 1);
-                    if (hl) density(A - 1, ml, 0);
-                    if (hr) density(A + ncol, mr, ncol + 1);
+                    load(A + t, cur);
+                    density(cur, m, t + 1);
+                    if (hl || hr) {
+                        T h[2][9];
+                        if (hl) {
+                            load(A - 1, h);
+                            density(h, ml, 0);
+                        }
+                        if (hr) {
+                            load(A + ncol, h);
+                            density(h, mr, ncol + 1);
+                        }
+                    }
                 }
             } else {
                 *abort_flag = 1;
@@ -220,7 +251,12 @@ __global__ void __launch_bounds__(RING_W, 1) k_ring2(const __grid_constant__ Fus
         }
         __syncthreads();
         aborted = *abort_flag != 0;
-        if (aborted) continue;
+        if (aborted) return;
+        // every thread has read row j's stage before the barrier
+        if (warp == 0 && j + R <= last) {
+            issue(j + R);
+            issued = j + R;
+        }
         if (act && j >= 2) {
             // rows below (sb), at (sc) and above (sa) the node of ring row j-1
             const int s_old = (j - 2) & 3, sc = (j - 1) & 3, s_new = slot;
@@ -229,14 +265,18 @@ __global__ void __launch_bounds__(RING_W, 1) k_ring2(const __grid_constant__ Fus
             const Stencil<T> st{{rho + sb * Q, rho + sc * Q, rho + sa * Q},
                                 {msk + sb * Q, msk + sc * Q, msk + sa * Q}, t + 1};
             const Nbr n = make_nbr(nx, x, xl, xr, yc, wrap1(yc - 1, ny), wrap1(yc + 1, ny));
-            const RingPops<S, T, P> f{pops + (size_t)((j - 1) % R) * 18 * P + A + t};
-            collide_push<S, T, FLAGS, WIDE>(a, f, st, n);
+            collide_push<S, T, FLAGS, WIDE>(a, prev, st, n);
         }
-        // the stage of row j-2 was last read before this iteration's barrier
-        if (warp == 0 && j >= 2 && j + R - 2 <= last) {
-            issue(j + R - 2);
-            issued = j + R - 2;
-        }
+    };
+    T Ab[2][9], Bb[2][9];
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+#pragma unroll
+        for (int i = 0; i < 9; ++i) Ab[k][i] = Bb[k][i] = T(0);
+    // two rows per trip so the register buffers swap roles instead of being copied
+    for (int j = 0; j <= last; j += 2) {
+        step_row(j, Ab, Bb);
+        if (j + 1 <= last) step_row(j + 1, Bb, Ab);
     }
     if (aborted && warp == 0 && lane == 0) {
         // let the copies still in flight land before the CTA's shared memory is released

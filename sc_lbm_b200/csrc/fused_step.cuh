@@ -98,6 +98,28 @@ __device__ __forceinline__ void feq_exact(double r, double ux, double uy, double
     fe[8] = rt2 * (1.0 + 3.0 * u8 + 4.5 * u8 * u8 - 1.5 * usq);
 }
 
+// A population as the lattice will hold it: FP16 storage rounds each value
+// (the remainder of mass_closing_rest is taken from the rounded values).
+template <typename S> __device__ __forceinline__ float stored_value(float v)
+{
+    if constexpr (sizeof(S) == 2) return __half2float(__float2half_rn(v));
+    else return v;
+}
+
+// Rest population of a shifted-form node chosen so that the node's stored
+// populations sum exactly (up to the rounding of this one value) to what the
+// collision conserves: the node's density deviation plus the volume force's
+// sum.  In exact arithmetic it equals the BGK rest population; in float, the
+// equilibrium weights rounded to float sum to 1 + 7.5e-9, and computing d*_0
+// like the others would scale every node's deviation by that factor each step
+// (a systematic mass drift of ~1e-4 over 20,000 steps).  v[1..8] are the
+// other post-collision values as they will be stored.
+__device__ __forceinline__ float mass_closing_rest(const float (&v)[9], float target)
+{
+    const float s = ((v[1] + v[3]) + (v[2] + v[4])) + ((v[5] + v[7]) + (v[6] + v[8]));
+    return target - s;
+}
+
 // shifted-form equilibrium deviation: w_i*(drho + rho*(3cu + 4.5cu^2 - 1.5u^2))
 __device__ __forceinline__ float feq_dev(int i, float drho, float r, float ux, float uy, float usq15)
 {
@@ -346,7 +368,6 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
             const float am = om * r[k], bm = om * dr[k];
             const float ux45 = 4.5f * ux, uy45 = 4.5f * uy;
             float v[9];
-            v[0] = fmaf(float(w_eq(0)), fmaf(am, -usq15, bm), omm * float(f[k][0]));
             auto pair = [&](int i, int j, float cu, float cu45) {
                 const float sq = fmaf(cu45, cu, -usq15);
                 v[i] = fmaf(float(w_eq(i)), fmaf(am, fmaf(3.f, cu, sq), bm), omm * float(f[k][i]));
@@ -357,10 +378,16 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
             pair(5, 7, ux + uy, ux45 + uy45);      // c = +-(1, 1)
             pair(6, 8, uy - ux, uy45 - ux45);      // c = +-(-1, 1)
 #pragma unroll
+            for (int i = 1; i < 9; ++i) {
+                // the force vector is zero for a component without a volume force
+                if constexpr (FORCE) v[i] += a.c[k].force[i];
+                v[i] = stored_value<S>(v[i]);
+            }
+            // the rest population closes the node's mass (sum_i d*_i = drho + sum_i F_i)
+            v[0] = mass_closing_rest(v, FORCE ? dr[k] + a.c[k].force_sum : dr[k]);
+#pragma unroll
             for (int i = 0; i < 9; ++i) {
                 float vi = v[i];
-                // the force vector is zero for a component without a volume force
-                if constexpr (FORCE) vi += a.c[k].force[i];
                 if constexpr (UNIFORM) vi = self_fluid ? vi : 0.f;
                 push_one<S, T, SOLID, WIDE>(a, k, i, vi, nf[i], n);
             }
@@ -837,12 +864,17 @@ __global__ void __launch_bounds__(256) k_fused1(const Fused1Args<S, T> a)
             const float ir = 1.0f / r;
             const float ux = jx * ir, uy = jy * ir;
             const float usq15 = 1.5f * fmaf(ux, ux, uy * uy);
+            float v[9];
 #pragma unroll
-            for (int i = 0; i < 9; ++i) {
-                float v = fmaf(a.c.omega, feq_dev(i, dr, r, ux, uy, usq15) - f[i], f[i]);
-                if (a.c.force_on) v += a.c.force[i];
-                out[i] = v;
+            for (int i = 1; i < 9; ++i) {
+                v[i] = fmaf(a.c.omega, feq_dev(i, dr, r, ux, uy, usq15) - f[i], f[i]);
+                if (a.c.force_on) v[i] += a.c.force[i];
+                v[i] = stored_value<S>(v[i]);
             }
+            // the rest population closes the node's mass (see mass_closing_rest)
+            v[0] = mass_closing_rest(v, a.c.force_on ? dr + a.c.force_sum : dr);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) out[i] = v[i];
         }
         const int xl = wrap1(x - 1, nx), xr = wrap1(x + 1, nx);
         const int yd = wrap1(y - 1, ny), yu = wrap1(y + 1, ny);

@@ -76,6 +76,7 @@ template <typename T> struct CompParams {
     T gs_neg;  // -1.0 * Gs (src/fluid.cpp:157)
     T rho_ref; // shift of the stored populations
     T force[9];
+    T force_sum; // sum_i force[i] (0 for the drivers' g/6 c_i forces)
     int force_on;
 };
 

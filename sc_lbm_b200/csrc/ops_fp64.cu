@@ -433,14 +433,15 @@ cudaError_t launch_batch2_async_fp64(const Fused2Args<double, double> *doms, con
 int async_resident_fp64() { return async_resident_ctas<double, double, 128, 3>(); }
 } // namespace sclbm
 
-// ring kernel, FP64 storage (-fmad=false keeps it bit-exact): 19 KB per stage;
-// solid lanes branch around the collision as in the FP64 register tile
+// ring kernel, FP64 storage (-fmad=false keeps it bit-exact): 19 KB per stage,
+// three stages beside the three CTAs per SM that the registers allow; solid
+// lanes branch around the collision as in the FP64 register tile
 #include "fused_ring.cuh"
 namespace sclbm {
 cudaError_t launch_ring2_fp64(const Fused2Args<double, double> &a, int stages, cudaStream_t s)
 {
-    if (stages < 0) return launch_ring2_any<double, double, 3, 0>(a, s);
-    if (stages > 0) return launch_ring2_any<double, double, 5, 0>(a, s);
-    return launch_ring2_any<double, double, 4, 0>(a, s);
+    if (stages < 0) return launch_ring2_any<double, double, 2, 0>(a, s);
+    if (stages > 0) return launch_ring2_any<double, double, 4, 0>(a, s);
+    return launch_ring2_any<double, double, 3, 0>(a, s);
 }
 } // namespace sclbm

@@ -42,7 +42,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 sys.path.insert(0, ROOT)
 
-B_LU = {"fp64": 289, "fp32s": 145, "fp16s": 73}
+B_LU = {"fp64": 289, "fp64_1ulp_twin": 289, "fp32s": 145, "fp16s": 73}
 
 
 def _env():
@@ -80,18 +80,93 @@ def _errors(a, b, fluid=None):
             "rms_over_mean": float(np.sqrt(np.mean(d * d)) / np.mean(np.abs(b)))}
 
 
+# --------------------------------------------------------------- error reports
+# Every shifted-form result states, per component, its density and velocity
+# error against the FP64 form (bit-exact with the reference) and its mass
+# drift.  The FP64 1-ulp twin starts with component 1's density one ulp
+# higher at every fluid node and is compared the same way: its error is what
+# the dynamics make of a rounding-sized difference, so a shifted form whose
+# error stays far above the twin's owes it to its storage, and one whose error
+# tracks the twin's amplification owes it to the physics.
+def twin_populations(f, mask=None):
+    """Populations whose node density is one ulp higher at fluid nodes: one
+    ulp of the density is added to the rest population (perturbing every f_i
+    by one ulp instead is lost in the density sum at tau = 1, where the
+    collision keeps nothing of f but its moments)."""
+    f = np.asarray(f, dtype=np.float64)
+    N = f.size // 9
+    g = f.copy()
+    rho = f.reshape(9, N).sum(axis=0)
+    bump = np.spacing(np.abs(rho))
+    if mask is not None:
+        bump = np.where(np.asarray(mask).ravel() != 0, bump, 0.0)
+    g[:N] += bump
+    return g
+
+
+def component_fields(d, c):
+    """Density and velocity of component c (u = sum_i f_i c_i / rho on fluid
+    nodes, Fluid::compute_velocities, src/fluid.cpp:186-200)."""
+    ux, uy = d.download_velocity(c)
+    return d.download_rho(c), ux, uy
+
+
+def field_errors(got, ref, fluid=None):
+    """Per component: max and RMS |drho| over the mean density, max |du| over
+    max |u_ref| and RMS |du| over RMS |u_ref| (|du| the vector difference)."""
+    r, ux, uy = got
+    r0, ux0, uy0 = ref
+    if fluid is not None:
+        r, ux, uy, r0, ux0, uy0 = (a[fluid] for a in (r, ux, uy, r0, ux0, uy0))
+    e = _errors(r, r0)
+    du = np.hypot(ux - ux0, uy - uy0)
+    u0 = np.hypot(ux0, uy0)
+    umax, urms = float(np.max(u0)), float(np.sqrt(np.mean(u0 * u0)))
+    return {"rho_max": e["max_over_mean"], "rho_rms": e["rms_over_mean"],
+            "u_max": float(np.max(du)) / umax if umax > 0 else float(np.max(du)),
+            "u_rms": float(np.sqrt(np.mean(du * du))) / urms if urms > 0 else
+            float(np.sqrt(np.mean(du * du))), "u_ref_max": umax}
+
+
+def compare_domains(doms, ref="fp64", fluid=None, ncomp=2):
+    """field_errors of every domain but the reference, component by component
+    (one component's fields on the host at a time)."""
+    out = {k: [] for k in doms if k != ref}
+    for c in range(ncomp):
+        base = component_fields(doms[ref], c)
+        for k, d in doms.items():
+            if k != ref:
+                out[k].append(field_errors(component_fields(d, c), base, fluid))
+    return out
+
+
+def mass_drift(d, m0, ncomp=2):
+    m1 = d.mass_momentum()
+    return [float((m1[3 * c] - m0[3 * c]) / m0[3 * c]) for c in range(ncomp)]
+
+
 # ----------------------------------------------------------------------------- configs
+PRECS = (("fp64", "FP64"), ("fp64_1ulp_twin", "FP64"), ("fp32s", "FP32_SHIFTED"),
+         ("fp16s", "FP16_SHIFTED"))
+
+
 def poiseuille(args):
     torch, sc, W, stream = _env()
     w = W.poiseuille()
     nx, ny = w["nx"], w["ny"]
     steps = 2000 if args.quick else 10000
-    p = sc.make_params(ncomp=1, tau=(w["tau"], 1.0), force=(w["force"], None))
-    d = sc.Domain(nx, ny, w["mask"], p, sc.FP64)
-    d.upload_f(0, w["f"])
-    ms = _timed(torch, stream, lambda: d.step(steps))
-    ux, _ = d.download_velocity(0)
-    rho = d.download_rho(0)
+    p = sc.make_params(ncomp=1, tau=(w["tau"], 1.0), rho_ref=(w["rho0"], 0.0),
+                       force=(w["force"], None))
+    doms, ms = {}, {}
+    for name, prec in PRECS:
+        d = sc.Domain(nx, ny, w["mask"], p, getattr(sc, prec))
+        d.upload_f(0, twin_populations(w["f"], w["mask"]) if "twin" in name else w["f"])
+        doms[name] = d
+    m0 = {k: d.mass_momentum() for k, d in doms.items()}
+    for k, d in doms.items():
+        ms[k] = _timed(torch, stream, lambda: d.step(steps))
+    ux, _ = doms["fp64"].download_velocity(0)
+    rho = doms["fp64"].download_rho(0)
     u = (ux.reshape(ny, nx))[:, nx // 2]
     # half-way bounce-back: walls midway between rows 0|1 and ny-2|ny-1
     nu = (w["tau"] - 0.5) / 3.0
@@ -101,9 +176,13 @@ def poiseuille(args):
     ua = w["g"] / (2 * nu * w["rho0"]) * (h * h - (y - yc) ** 2)
     fl = slice(1, ny - 1)
     err = float(np.linalg.norm(u[fl] - ua[fl]) / np.linalg.norm(ua[fl]))
-    return {"config": "poiseuille 200x50 FP64", "steps": steps, "ms": round(ms, 2),
+    fluid = np.asarray(w["mask"]).ravel() != 0
+    return {"config": "poiseuille 200x50 FP64 (shifted forms and twin alongside)", "steps": steps,
+            "ms": {k: round(v, 2) for k, v in ms.items()},
             "u_max": float(u.max()), "u_max_analytic": float(ua.max()),
-            "l2_rel_error_vs_analytic": err, "mean_rho": float(rho.reshape(ny, nx)[fl].mean())}
+            "l2_rel_error_vs_analytic": err, "mean_rho": float(rho.reshape(ny, nx)[fl].mean()),
+            "errors_vs_fp64": compare_domains(doms, fluid=fluid, ncomp=1),
+            "mass_drift": {k: mass_drift(d, m0[k], 1) for k, d in doms.items()}}
 
 
 def _laplace_stats(rho1, rho2, nx, ny, G):
@@ -125,25 +204,31 @@ def laplace(args):
     steps = 4000 if args.quick else 20000
     out = {"config": "laplace 256x256, G=0.9, radii 20-40, one batch per precision",
            "steps": steps}
-    for prec, name in ((sc.FP64, "fp64"), (sc.FP32_SHIFTED, "fp32s")):
-        ws = [W.laplace(r) for r in radii]
+    ws = [W.laplace(r) for r in radii]
+    sets = {}
+    for name, prec in PRECS:
         doms = []
         for w in ws:
             rr = tuple(float(w[k].reshape(9, -1).sum(0).mean()) for k in ("f1", "f2"))
-            d = sc.Domain(w["nx"], w["ny"], w["mask"], W.params_of(w, sc, rho_ref=rr), prec)
-            d.upload_f(0, w["f1"])
+            d = sc.Domain(w["nx"], w["ny"], w["mask"], W.params_of(w, sc, rho_ref=rr),
+                          getattr(sc, prec))
+            d.upload_f(0, twin_populations(w["f1"]) if "twin" in name else w["f1"])
             d.upload_f(1, w["f2"])
             doms.append(d)
+        m0 = [d.mass_momentum() for d in doms]
         b = sc.Batch(doms)
         ms = _timed(torch, stream, lambda: b.step(steps))
+        del b
+        sets[name] = doms
         rows = []
-        for w, d in zip(ws, doms):
+        for w, d, a in zip(ws, doms, m0):
             r1, r2 = d.download_rho(0), d.download_rho(1)
             (u1x, u1y), (u2x, u2y) = d.download_velocity(0), d.download_velocity(1)
             jx, jy = r1 * u1x + r2 * u2x, r1 * u1y + r2 * u2y
             umax = float(np.max(np.hypot(jx, jy) / (r1 + r2)))
             R, dp = _laplace_stats(r1, r2, w["nx"], w["ny"], w["G"])
-            rows.append({"R0": w["radius"], "R": R, "dp": dp, "max_spurious_u": umax})
+            rows.append({"R0": w["radius"], "R": R, "dp": dp, "max_spurious_u": umax,
+                         "mass_drift": mass_drift(d, a)})
         inv = np.array([1.0 / r["R"] for r in rows])
         dps = np.array([r["dp"] for r in rows])
         A = np.vstack([inv, np.ones_like(inv)]).T
@@ -153,9 +238,15 @@ def laplace(args):
         out[name] = {"droplets": rows, "surface_tension": float(sigma), "intercept": float(c0),
                      "fit_r2": r2, "ms": round(ms, 2),
                      "mlups": round(sum(d.N for d in doms) * steps / (ms * 1e-3) / 1e6, 1)}
-        del b, doms
-    out["surface_tension_rel_diff_fp32s"] = abs(out["fp32s"]["surface_tension"] /
-                                                out["fp64"]["surface_tension"] - 1)
+    # field errors of every droplet against its FP64 run
+    for name in ("fp64_1ulp_twin", "fp32s", "fp16s"):
+        per = [compare_domains({"fp64": sets["fp64"][i], name: sets[name][i]})[name]
+               for i in range(len(ws))]
+        out[name]["errors_vs_fp64"] = per
+        out[name]["worst_vs_fp64"] = {q: max(c[q] for p_ in per for c in p_)
+                                      for q in ("rho_max", "rho_rms", "u_max", "u_rms")}
+        out[name]["surface_tension_rel_diff"] = abs(out[name]["surface_tension"] /
+                                                    out["fp64"]["surface_tension"] - 1)
     return out
 
 
@@ -167,11 +258,11 @@ def drainage(args):
     total = 10000 if args.quick else 50000
     checkpoints = [c for c in (100, 1000, 10000, 50000) if c <= total]
     doms = {}
-    for prec, name in ((sc.FP64, "fp64"), (sc.FP32_SHIFTED, "fp32s"), (sc.FP16_SHIFTED, "fp16s")):
+    for name, prec in PRECS:
         rr = (float(w["f1"].reshape(9, -1).sum(0)[fluid].mean()),
               float(w["f2"].reshape(9, -1).sum(0)[fluid].mean()))
-        d = sc.Domain(nx, ny, w["mask"], W.params_of(w, sc, rho_ref=rr), prec)
-        d.upload_f(0, w["f1"])
+        d = sc.Domain(nx, ny, w["mask"], W.params_of(w, sc, rho_ref=rr), getattr(sc, prec))
+        d.upload_f(0, twin_populations(w["f1"], w["mask"]) if "twin" in name else w["f1"])
         d.upload_f(1, w["f2"])
         doms[name] = d
     m0 = {k: d.mass_momentum() for k, d in doms.items()}
@@ -183,16 +274,13 @@ def drainage(args):
         for k, d in doms.items():
             ms_tot[k] += _timed(torch, stream, lambda: d.step(cp - done))
         done = cp
-        ref = [doms["fp64"].download_rho(c) for c in range(2)]
-        row = {}
-        for k in ("fp32s", "fp16s"):
-            rho = [doms[k].download_rho(c) for c in range(2)]
-            row[k] = [_errors(rho[c], ref[c], fluid) for c in range(2)]
-            row[k + "_saturation1"] = float(np.mean(rho[0][fluid] > rho[1][fluid]))
-        row["fp64_saturation1"] = float(np.mean(ref[0][fluid] > ref[1][fluid]))
+        row = {"errors_vs_fp64": compare_domains(doms, fluid=fluid),
+               "mass_drift": {k: mass_drift(d, m0[k]) for k, d in doms.items()}}
+        for k, d in doms.items():
+            r0, r1 = d.download_rho(0), d.download_rho(1)
+            row[k + "_saturation1"] = float(np.mean(r0[fluid] > r1[fluid]))
         out["checkpoints"][str(cp)] = row
-    out["mass_drift"] = {k: [float((d.mass_momentum()[3 * c] - m0[k][3 * c]) / m0[k][3 * c])
-                             for c in range(2)] for k, d in doms.items()}
+    out["mass_drift"] = {k: mass_drift(d, m0[k]) for k, d in doms.items()}
     out["mlups"] = {k: round(N * total / (ms * 1e-3) / 1e6, 1) for k, ms in ms_tot.items()}
     return out
 
@@ -218,12 +306,13 @@ def ensemble(args):
     out = {"config": f"ensemble of {n} seeded porous domains, one batch per precision",
            "steps": steps, "porosity_mean": float(np.mean([m["porosity"] for m in members])),
            "generation_s": round(gen_s, 1)}
-    rho, finite = {}, {}
-    for prec, name in ((sc.FP32_SHIFTED, "fp32s"), (sc.FP64, "fp64")):
+    finite, sets = {}, {}
+    for name, prec in (("fp32s", "FP32_SHIFTED"), ("fp64", "FP64"), ("fp64_1ulp_twin", "FP64"),
+                       ("fp16s", "FP16_SHIFTED")):
         doms = []
         for m in members:
-            d = sc.Domain(m["nx"], m["ny"], m["mask"], W.params_of(m, sc), prec)
-            d.upload_f(0, m["f1"])
+            d = sc.Domain(m["nx"], m["ny"], m["mask"], W.params_of(m, sc), getattr(sc, prec))
+            d.upload_f(0, twin_populations(m["f1"], m["mask"]) if "twin" in name else m["f1"])
             d.upload_f(1, m["f2"])
             doms.append(d)
         nodes = sum(d.N for d in doms)
@@ -241,24 +330,32 @@ def ensemble(args):
             except sc.capi.SclbmNonFinite:
                 ok.append(False)
         finite[name] = ok
-        rho[name] = [d.download_rho(0) if good else None for d, good in zip(doms, ok)]
+        sets[name] = doms
         out[name] = {"mlups": round(nodes * steps / (ms * 1e-3) / 1e6, 1), "tiles": ntiles,
                      "ctas": grid, "nodes": nodes, "non_finite_domains": int(len(ok) - sum(ok)),
                      "max_mass_drift_finite": float(max(drift)) if drift else None}
-        del b, doms
+        del b
     bad = [k for k in range(n) if not finite["fp32s"][k] or not finite["fp64"][k]]
     out["non_finite_params"] = [
         {"k": k, "nx": members[k]["nx"], "ny": members[k]["ny"], "tau": members[k]["tau"][0],
          "G": members[k]["G"], "Gs": members[k]["Gs"][0], "porosity": members[k]["porosity"],
          "fp32s_finite": finite["fp32s"][k], "fp64_finite": finite["fp64"][k]} for k in bad[:20]]
-    errs = []
-    for k in range(n):
-        if finite["fp32s"][k] and finite["fp64"][k]:
+    # field errors over the members that stay finite in every form (the
+    # others go non-finite in FP64 too, at the reference's own step)
+    stable = [k for k in range(n) if all(finite[x][k] for x in finite)]
+    out["stable_members"] = len(stable)
+    for name in ("fp64_1ulp_twin", "fp32s", "fp16s"):
+        per = []
+        for k in stable:
             fl = np.asarray(members[k]["mask"]).ravel() != 0
-            a, b_ = rho["fp32s"][k][fl], rho["fp64"][k][fl]
-            errs.append(float(np.max(np.abs(a - b_)) / np.mean(np.abs(b_))))
-    out["fp32s_rho1_max_over_mean_vs_fp64"] = {
-        "median": float(np.median(errs)), "max": float(np.max(errs))} if errs else None
+            e = compare_domains({"fp64": sets["fp64"][k], name: sets[name][k]}, fluid=fl)[name]
+            per.append({q: max(c[q] for c in e) for q in ("rho_max", "rho_rms", "u_max", "u_rms")})
+        out[name]["errors_vs_fp64_stable_members"] = {
+            q: {"median": float(np.median([p_[q] for p_ in per])),
+                "p90": float(np.percentile([p_[q] for p_ in per], 90)),
+                "max": float(np.max([p_[q] for p_ in per]))}
+            for q in ("rho_max", "rho_rms", "u_max", "u_rms")} if per else None
+    del sets
     # single large domains of the same storage for the efficiency ratio
     D = sc.Domain(4096, 4096, np.ones(4096 * 4096, np.int32),
                   sc.make_params(ncomp=2, g_fluid=(1.2, 1.2), rho_ref=(1.0, 1.0)), sc.FP32_SHIFTED)
@@ -288,11 +385,14 @@ def spinodal(args):
     steps = 1000 if args.quick else 5000
     peak = _peak()
     doms = {}
-    for prec, name in ((sc.FP64, "fp64"), (sc.FP32_SHIFTED, "fp32s"), (sc.FP16_SHIFTED, "fp16s")):
+    for name, prec in PRECS:
         d = sc.Domain(nx, ny, np.ones(N, np.int32),
-                      sc.make_params(ncomp=2, g_fluid=(1.2, 1.2), rho_ref=(1.0, 1.0)), prec)
+                      sc.make_params(ncomp=2, g_fluid=(1.2, 1.2), rho_ref=(1.0, 1.0)),
+                      getattr(sc, prec))
         d.init_noise(0, 1.0, 0.01, 101)
         d.init_noise(1, 1.0, 0.01, 102)
+        if "twin" in name:
+            d.upload_f(0, twin_populations(d.download_f(0)))
         doms[name] = d
     m0 = {k: d.mass_momentum() for k, d in doms.items()}
     out = {"config": f"spinodal {nx}x{ny} periodic, G=1.2, rho=1+-1%", "steps": steps,
@@ -302,12 +402,9 @@ def spinodal(args):
         for k, d in doms.items():
             ms[k] += _timed(torch, stream, lambda: d.step(cp - done))
         done = cp
-        ref = [doms["fp64"].download_rho(c) for c in range(2)]
-        acc[str(cp)] = {k: [_errors(doms[k].download_rho(c), ref[c]) for c in range(2)]
-                        for k in ("fp32s", "fp16s")}
-    out["accuracy_vs_fp64"] = acc
-    out["mass_drift"] = {k: [float((d.mass_momentum()[3 * c] - m0[k][3 * c]) / m0[k][3 * c])
-                             for c in range(2)] for k, d in doms.items()}
+        acc[str(cp)] = compare_domains(doms)
+    out["errors_vs_fp64"] = acc
+    out["mass_drift"] = {k: mass_drift(d, m0[k]) for k, d in doms.items()}
     out["mlups"] = {k: round(N * steps / (t * 1e-3) / 1e6, 1) for k, t in ms.items()}
     out["hbm_frac"] = {k: round(B_LU[k] * N * steps / (t * 1e-3) / 1e9 / peak, 4)
                        for k, t in ms.items()}
@@ -324,14 +421,16 @@ def contact(args):
     steps = 5000 if args.quick else 30000
     out = {"config": "contact angles 400x306, droplet on a 341x20 shelf, G=0.9, "
                      "Gs_droplet -0.4..0.4, one batch per precision", "steps": steps}
-    for prec, name in ((sc.FP64, "fp64"), (sc.FP32_SHIFTED, "fp32s")):
-        ws = [W.contact_angle(g) for g in gs_values]
+    ws = [W.contact_angle(g) for g in gs_values]
+    sets = {}
+    for name, prec in PRECS:
         doms = []
         for w in ws:
             fl = np.asarray(w["mask"]).ravel() != 0
             rr = tuple(float(w[k].reshape(9, -1).sum(0)[fl].mean()) for k in ("f1", "f2"))
-            d = sc.Domain(w["nx"], w["ny"], w["mask"], W.params_of(w, sc, rho_ref=rr), prec)
-            d.upload_f(0, w["f1"])
+            d = sc.Domain(w["nx"], w["ny"], w["mask"], W.params_of(w, sc, rho_ref=rr),
+                          getattr(sc, prec))
+            d.upload_f(0, twin_populations(w["f1"], w["mask"]) if "twin" in name else w["f1"])
             d.upload_f(1, w["f2"])
             doms.append(d)
         m0 = [d.mass_momentum() for d in doms]
@@ -353,10 +452,18 @@ def contact(args):
                      all(th[i] < th[i + 1] for i in range(len(th) - 1)),
                      "ms": round(ms, 2),
                      "mlups": round(sum(d.N for d in doms) * steps / (ms * 1e-3) / 1e6, 1)}
-        del b, doms
-    a, b_ = out["fp64"]["theta_deg"], out["fp32s"]["theta_deg"]
-    out["max_abs_theta_diff_fp32s_deg"] = max(
-        (abs(x - y) for x, y in zip(a, b_) if x is not None and y is not None), default=None)
+        del b
+        sets[name] = doms
+    for name in ("fp64_1ulp_twin", "fp32s", "fp16s"):
+        a, b_ = out["fp64"]["theta_deg"], out[name]["theta_deg"]
+        out[name]["max_abs_theta_diff_deg"] = max(
+            (abs(x - y) for x, y in zip(a, b_) if x is not None and y is not None), default=None)
+        per = [compare_domains({"fp64": sets["fp64"][i], name: sets[name][i]},
+                               fluid=np.asarray(ws[i]["mask"]).ravel() != 0)[name]
+               for i in range(len(ws))]
+        out[name]["errors_vs_fp64"] = per
+        out[name]["worst_vs_fp64"] = {q: max(c[q] for p_ in per for c in p_)
+                                      for q in ("rho_max", "rho_rms", "u_max", "u_rms")}
     return out
 
 

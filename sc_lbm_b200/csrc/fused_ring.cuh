@@ -1,15 +1,17 @@
 // fused_ring.cuh -- the fused two-component step with its population rows
-// streamed into a shared-memory ring by bulk asynchronous copies (the TMA
-// engine: cp.async.bulk global -> shared, completion counted in bytes on an
-// mbarrier per ring stage).
+// streamed into a shared-memory ring by the TMA engine (cp.async.bulk.tensor:
+// one 3-D box per component and row -- the row segment of all nine
+// directions -- completion counted in bytes on an mbarrier per ring stage).
 //
 // Why.  The register-tile kernel (fused_step.cuh) keeps at most one row of
 // loads in flight per warp, and the registers that hold them cap residency;
 // its FP32 and FP16 forms wait on load latency.  Here the bytes in flight do
 // not live in registers: each CTA keeps R whole population rows on their way
 // into shared memory while its threads reduce one row and collide the one
-// before it.  One copy per population array and row replaces eighteen
-// per-thread loads and their address arithmetic.
+// before it.  Two tensor copies per row replace eighteen per-thread loads
+// and their address arithmetic (eighteen 1-D bulk copies per row, one per
+// population array, were measured slower than the register tile: the copy
+// engine's per-copy cost dominated at 300-1000 bytes a copy).
 //
 // Work decomposition.  A CTA of RING_W threads owns a strip of RING_W interior
 // columns and a band of rows; the bands split every strip at the same rows
@@ -19,9 +21,12 @@
 // and the second read hits L2.
 //
 // Ring.  Row j of a band (j = 0 .. nrow+1, halo rows included) lands in stage
-// j % R: 18 arrays (component k, direction i) of P = RING_W + 2A elements,
+// j % R: per component a box of 9 directions x P = RING_W + 2A elements,
 // lattice columns xb - A .. xb + RING_W + A - 1, where A elements make 16 bytes
-// (copies start and end on 16-byte boundaries: nx must be a multiple of A).
+// (a box's first column must start on a 16-byte boundary: nx must be a
+// multiple of A).  Columns outside the lattice arrive as zeros; where a strip
+// touches the lattice's left or right edge, the periodic halo column comes
+// from a second, A-column box at the other edge.
 // Iteration j waits for row j, reads each thread's column into registers and
 // reduces it to both components' densities (density ring in shared memory,
 // one __syncthreads); the stage is then free and is refilled at once with row
@@ -35,6 +40,8 @@
 // sets *a.status and the CTA skips the rest of its band (no hang); the
 // domain's monitor reports the flag.
 #pragma once
+#include <cuda.h>
+
 #include "fused_step.cuh"
 
 namespace sclbm {
@@ -47,15 +54,20 @@ template <typename S> constexpr int ring_pad() { return 16 / (int)sizeof(S); }
 
 template <typename S, typename T, int R> struct RingLayout {
     static constexpr int A = ring_pad<S>();
-    static constexpr int P = RING_W + 2 * A;                    // elements per array row
-    static constexpr int Q = RING_W + 2;                        // density ring columns
-    static constexpr size_t stage = size_t(18) * P * sizeof(S); // multiple of 16
+    static constexpr int P = RING_W + 2 * A; // box columns
+    static constexpr int Q = RING_W + 2;     // density ring columns
+    // tensor-copy destinations start on 128-byte boundaries
+    static constexpr size_t comp = (size_t(9) * P * sizeof(S) + 127) & ~size_t(127);
+    static constexpr size_t halo = 256; // one A-column box of one component (144 bytes)
+    static constexpr size_t stage = 2 * comp + 4 * halo; // components, then halos [side][k]
     static constexpr size_t pops = size_t(R) * stage;
     static constexpr size_t rho = size_t(4) * Q * sizeof(V2<T>);
     static constexpr size_t msk = size_t(4) * Q;
     static constexpr size_t bars = (pops + rho + msk + 15) & ~size_t(15);
-    static constexpr size_t bytes = bars + size_t(R) * 8 + 16;
-    static_assert(stage % 16 == 0, "ring stages must keep 16-byte alignment");
+    static constexpr size_t bytes = bars + size_t(R) * 8 + 16 + 128; // + base alignment
+    static constexpr uint32_t CE = (uint32_t)(comp / sizeof(S));     // component stride, elements
+    static_assert(comp % 128 == 0 && stage % 128 == 0, "tensor-copy alignment");
+    static_assert(size_t(9) * A * sizeof(S) <= halo, "halo box");
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
@@ -87,18 +99,32 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
                  : "memory");
     return ok != 0;
 }
-// bulk copy of `bytes` (multiple of 16) from global src to shared dst (both
-// 16-byte aligned), completing on mbarrier `bar`; no multicast
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
+// one 3-D box of a tiled tensor map into shared memory (dst 128-byte aligned),
+// completing on mbarrier `bar`; coordinates in elements (x may be negative or
+// past the end: those elements arrive as zeros); no multicast
+__device__ __forceinline__ void tensor_g2s_3d(uint32_t dst, const void *map, int x, int y, int z,
+                                              uint32_t bar)
 {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-        "l"(src), "r"(bytes), "r"(bar)
-        : "memory");
+    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+                 "l"(map), "r"(x), "r"(y), "r"(z), "r"(bar)
+                 : "memory");
 }
 
+// tiled tensor map over [dim[2]][dim[1]][dim[0]] (no swizzle, zero fill,
+// 256-byte L2 promotion); 0 on success (tensor_map.cpp)
+int encode_tensor_map(CUtensorMap *m, CUtensorMapDataType dt, unsigned rank, void *base,
+                      const cuuint64_t *dim, const cuuint64_t *stride_bytes, const cuuint32_t *box,
+                      const cuuint32_t *elem_strides);
+
+// The four tensor maps of one launch: per component the row box (P x 1 x 9)
+// and the halo box (A x 1 x 9) over the input populations [9][ny][nx].
+struct RingMaps {
+    CUtensorMap row[2], halo[2];
+};
+
 // resident CTAs per SM the register cap aims at (the ring's shared memory
-// allows at least as many): the register tile's figures, six for FP32
+// allows about as many): the register tile's figures, six for FP32
 // arithmetic (five in the uniform solid form, which spills at 80 registers),
 // three for FP64
 template <typename T, int FLAGS> constexpr int ring_min_ctas()
@@ -109,13 +135,15 @@ template <typename T, int FLAGS> constexpr int ring_min_ctas()
 // One band of one strip per CTA; band b covers rows [b*ny/bands, (b+1)*ny/bands).
 template <typename S, typename T, int FLAGS, int R, bool WIDE>
 __global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS>()))
-    k_ring2(const __grid_constant__ Fused2Args<S, T> a, int bands)
+    k_ring2(const __grid_constant__ Fused2Args<S, T> a, const __grid_constant__ RingMaps maps, int bands)
 {
     using L = RingLayout<S, T, R>;
     constexpr int A = L::A, P = L::P, Q = L::Q;
+    constexpr uint32_t CE = L::CE;
     constexpr bool SOLID = (FLAGS & KF_SOLID) != 0;
-    extern __shared__ __align__(128) unsigned char ring_smem[];
-    S *pops = reinterpret_cast<S *>(ring_smem);
+    extern __shared__ __align__(128) unsigned char ring_raw[];
+    unsigned char *ring_smem =
+        reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(ring_raw) + 127) & ~uintptr_t(127));
     V2<T> *rho = reinterpret_cast<V2<T> *>(ring_smem + L::pops);
     uint8_t *msk = ring_smem + L::pops + L::rho;
     uint64_t *bars = reinterpret_cast<uint64_t *>(ring_smem + L::bars);
@@ -145,27 +173,30 @@ __global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS>()))
     }
     __syncthreads();
 
-    // warp 0 requests row j: lanes 0..17 copy one population array each
-    const uint32_t row_bytes = 18u * (uint32_t)(ncol + 2 * A) * (uint32_t)sizeof(S);
-    const bool one_copy = xb >= A && xb + ncol + A <= nx;
-    const int left_src = xb >= A ? xb - A : nx - A;        // A columns left of the strip
-    const int right_src = xb + ncol == nx ? 0 : xb + ncol; // A columns right of it
+    // the halo column left (right) of the strip wraps around the lattice edge:
+    // it comes from an A-column box at the other edge
+    const bool wrap_l = xb == 0, wrap_r = xb + ncol == nx;
+    const uint32_t box_bytes = 9u * (uint32_t)P * (uint32_t)sizeof(S);
+    const uint32_t halo_bytes = 9u * (uint32_t)A * (uint32_t)sizeof(S);
+    const uint32_t row_bytes = 2u * (box_bytes + (wrap_l ? halo_bytes : 0u) + (wrap_r ? halo_bytes : 0u));
+    auto stage_at = [&](int st) { return ring_smem + (size_t)st * L::stage; };
+    // lane 0 of warp 0 requests row j: one box per component (+ halo boxes)
     auto issue = [&](int j) {
+        if (lane != 0) return;
         const int st = j % R;
         const uint32_t bar = smem_addr(&bars[st]);
-        if (lane == 0) mbar_expect_tx(bar, row_bytes);
-        __syncwarp();
-        if (lane < 18) {
-            const int k = lane >= 9 ? 1 : 0, i = lane - 9 * k;
-            const S *row = a.fin[k] + (size_t)i * a.N + (size_t)gy(j) * (size_t)nx;
-            S *dst = pops + ((size_t)st * 18 + lane) * P;
-            if (one_copy) {
-                bulk_g2s(smem_addr(dst), row + (xb - A), (uint32_t)((ncol + 2 * A) * sizeof(S)), bar);
-            } else {
-                bulk_g2s(smem_addr(dst), row + left_src, (uint32_t)(A * sizeof(S)), bar);
-                bulk_g2s(smem_addr(dst + A), row + xb, (uint32_t)(ncol * sizeof(S)), bar);
-                bulk_g2s(smem_addr(dst + A + ncol), row + right_src, (uint32_t)(A * sizeof(S)), bar);
-            }
+        const uint32_t sb = smem_addr(stage_at(st));
+        const int y = gy(j);
+        mbar_expect_tx(bar, row_bytes);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            tensor_g2s_3d(sb + k * (uint32_t)L::comp, &maps.row[k], xb - A, y, 0, bar);
+            if (wrap_l)
+                tensor_g2s_3d(sb + 2 * (uint32_t)L::comp + (0 + k) * (uint32_t)L::halo, &maps.halo[k],
+                              nx - A, y, 0, bar);
+            if (wrap_r)
+                tensor_g2s_3d(sb + 2 * (uint32_t)L::comp + (2 + k) * (uint32_t)L::halo, &maps.halo[k], 0,
+                              y, 0, bar);
         }
     };
     auto wait_row = [&](int j) {
@@ -177,11 +208,16 @@ __global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS>()))
     };
 
     int issued = -1; // last row requested (warp 0's view)
-    if (warp == 0)
+    if (warp == 0) {
+        if (lane == 0) {
+            asm volatile("prefetch.tensormap [%0];" ::"l"(&maps.row[0]) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(&maps.row[1]) : "memory");
+        }
         for (int j = 0; j < R && j <= last; ++j) {
             issue(j);
             issued = j;
         }
+    }
 
     // masks of the next row, loaded one row ahead
     uint8_t mn = 1, mnl = 1, mnr = 1;
@@ -209,7 +245,10 @@ __global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS>()))
         if (!aborted) {
             if (wait_row(j)) {
                 consumed = j;
-                const S *stg = pops + (size_t)(j % R) * 18 * P;
+                const unsigned char *sg = stage_at(j % R);
+                const S *stg = reinterpret_cast<const S *>(sg);
+                const S *hlp = reinterpret_cast<const S *>(sg + 2 * L::comp);            // [k][9][A]
+                const S *hrp = reinterpret_cast<const S *>(sg + 2 * L::comp + 2 * L::halo);
                 auto density = [&](const T(&f)[2][9], uint8_t mm, int q) {
                     T r[2];
 #pragma unroll
@@ -223,23 +262,27 @@ __global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS>()))
                     rho[slot * Q + q] = Vec2<T>::make(r[0], r[1]);
                     msk[slot * Q + q] = SOLID ? mm : 1;
                 };
-                auto load = [&](int col, T(&f)[2][9]) {
+                // f[k][i] from a box of component stride cs, direction stride ds
+                auto load = [&](const S *p, uint32_t cs, int ds, int col, T(&f)[2][9]) {
 #pragma unroll
                     for (int k = 0; k < 2; ++k)
 #pragma unroll
-                        for (int i = 0; i < 9; ++i) f[k][i] = T(stg[(k * 9 + i) * P + col]);
+                        for (int i = 0; i < 9; ++i) f[k][i] = T(p[k * cs + i * ds + col]);
                 };
+                constexpr uint32_t HE = (uint32_t)(L::halo / sizeof(S));
                 if (act) {
-                    load(A + t, cur);
+                    load(stg, CE, P, A + t, cur);
                     density(cur, m, t + 1);
                     if (hl || hr) {
                         T h[2][9];
                         if (hl) {
-                            load(A - 1, h);
+                            if (wrap_l) load(hlp, HE, A, A - 1, h);
+                            else load(stg, CE, P, A - 1, h);
                             density(h, ml, 0);
                         }
                         if (hr) {
-                            load(A + ncol, h);
+                            if (wrap_r) load(hrp, HE, A, 0, h);
+                            else load(stg, CE, P, A + ncol, h);
                             density(h, mr, ncol + 1);
                         }
                     }
@@ -284,6 +327,26 @@ __global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS>()))
     }
 }
 
+// tensor maps of the input populations of both components (host)
+template <typename S, typename T, int R>
+inline cudaError_t ring_maps(const Fused2Args<S, T> &a, RingMaps &m)
+{
+    using L = RingLayout<S, T, R>;
+    const CUtensorMapDataType dt = sizeof(S) == 8   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                   : sizeof(S) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                                    : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    const cuuint64_t dim[3] = {(cuuint64_t)a.nx, (cuuint64_t)a.ny, 9};
+    const cuuint64_t stride[2] = {(cuuint64_t)a.nx * sizeof(S), (cuuint64_t)a.N * sizeof(S)};
+    const cuuint32_t row_box[3] = {(cuuint32_t)L::P, 1, 9}, halo_box[3] = {(cuuint32_t)L::A, 1, 9};
+    const cuuint32_t es[3] = {1, 1, 1};
+    for (int k = 0; k < 2; ++k) {
+        int rc = encode_tensor_map(&m.row[k], dt, 3, (void *)a.fin[k], dim, stride, row_box, es);
+        if (!rc) rc = encode_tensor_map(&m.halo[k], dt, 3, (void *)a.fin[k], dim, stride, halo_box, es);
+        if (rc) return cudaErrorInvalidValue;
+    }
+    return cudaSuccess;
+}
+
 template <typename S, typename T, int FLAGS, int R, bool WIDE>
 inline cudaError_t launch_ring2_f(const Fused2Args<S, T> &a, cudaStream_t s)
 {
@@ -304,7 +367,10 @@ inline cudaError_t launch_ring2_f(const Fused2Args<S, T> &a, cudaStream_t s)
     // one wave: as many bands as resident CTAs allow, at least 4 rows each
     int bands = std::max(1, resident / strips);
     bands = std::min(bands, std::max(1, a.ny / 4));
-    kern<<<dim3(strips, bands), RING_W, L::bytes, s>>>(a, bands);
+    RingMaps maps;
+    const cudaError_t em = ring_maps<S, T, R>(a, maps);
+    if (em != cudaSuccess) return em;
+    kern<<<dim3(strips, bands), RING_W, L::bytes, s>>>(a, maps, bands);
     return cudaGetLastError();
 }
 

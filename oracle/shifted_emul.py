@@ -12,9 +12,9 @@ path:
         S = sum over solid neighbours of w c (the solid-force sums)
     d_eq_i = w_i (drho + rho (3 c.u + 4.5 (c.u)^2 - 1.5 u^2))
     d*_i   = d_i + omega (d_eq_i - d_i) [+ F_i]     (i = 1..8, rounded to storage)
-    d*_0   = drho [+ sum_i F_i] - sum_{i>=1} d*_i     (the rest population closes
-             the node's mass, as the kernel does: equal to the BGK value in
-             exact arithmetic)
+    d*_0   = d_0 + sum_{i>=1} (d_i - d*_i) [+ sum_i F_i]   (the rest population
+             closes the node's mass, as the kernel does: equal to the BGK
+             value in exact arithmetic)
 
 followed by push streaming with half-way bounce-back.  The tests use it as
 the checker of the GPU float path (same rounding regime, so agreement is
@@ -64,7 +64,7 @@ def step(d, mask, p, store=np.float32, compute=np.float32):
         io = T(1) / om[k]
         u = [uc[a] + F[k][a] * (io / r[k]) + T(-p["Gs"][k]) * S[a] * io for a in range(2)]
         usq = T(1.5) * (u[0] * u[0] + u[1] * u[1])
-        rest = drho[k] + (sum(T(p["force"][k][i]) for i in range(9))
+        rest = x[k][0] + (sum(T(p["force"][k][i]) for i in range(9))
                           if p["force"][k] is not None else T(0))
         for i in range(1, 9):
             cu = T(CX[i]) * u[0] + T(CY[i]) * u[1]
@@ -74,7 +74,7 @@ def step(d, mask, p, store=np.float32, compute=np.float32):
                 v = v + T(p["force"][k][i])
             v = np.where(mask, v, T(0)).astype(store).astype(T)
             out[k][i] = v
-            rest = rest - v
+            rest = rest + (x[k][i] - v)
         out[k][0] = np.where(mask, rest, T(0))
     out = out.astype(store)
     new = np.zeros_like(out)

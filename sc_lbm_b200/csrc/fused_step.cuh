@@ -107,17 +107,25 @@ template <typename S> __device__ __forceinline__ float stored_value(float v)
 }
 
 // Rest population of a shifted-form node chosen so that the node's stored
-// populations sum exactly (up to the rounding of this one value) to what the
-// collision conserves: the node's density deviation plus the volume force's
-// sum.  In exact arithmetic it equals the BGK rest population; in float, the
-// equilibrium weights rounded to float sum to 1 + 7.5e-9, and computing d*_0
-// like the others would scale every node's deviation by that factor each step
-// (a systematic mass drift of ~1e-4 over 20,000 steps).  v[1..8] are the
-// other post-collision values as they will be stored.
-__device__ __forceinline__ float mass_closing_rest(const float (&v)[9], float target)
+// populations sum to what the collision conserves -- the incoming
+// populations' sum plus the volume force's sum -- up to the rounding of this
+// one value:  d*_0 = d_0 + sum_{i>=1} (d_i - d*_i) [+ sum_i F_i].  In exact
+// arithmetic it equals the BGK rest population.  In float it closes two
+// systematic leaks: the equilibrium weights rounded to float sum to
+// 1 + 7.5e-9 (computing d*_0 like the others scaled every node's deviation by
+// that each step, ~1e-4 of the mass over 20,000 steps), and the node density
+// is a rounded nine-term sum whose error is the same at every node of a
+// uniform bulk.  Near equilibrium d_i - d*_i is small and nearly exact, so
+// the remainder is accurate.  d: incoming values; v[1..8]: the outgoing
+// values as they will be stored.
+template <typename Row>
+__device__ __forceinline__ float mass_closing_rest(const Row &d, const float (&v)[9], float force_sum)
 {
-    const float s = ((v[1] + v[3]) + (v[2] + v[4])) + ((v[5] + v[7]) + (v[6] + v[8]));
-    return target - s;
+    const float a = (float(d[1]) - v[1]) + (float(d[3]) - v[3]);
+    const float b = (float(d[2]) - v[2]) + (float(d[4]) - v[4]);
+    const float c = (float(d[5]) - v[5]) + (float(d[7]) - v[7]);
+    const float e = (float(d[6]) - v[6]) + (float(d[8]) - v[8]);
+    return float(d[0]) + (((a + b) + (c + e)) + force_sum);
 }
 
 // shifted-form equilibrium deviation: w_i*(drho + rho*(3cu + 4.5cu^2 - 1.5u^2))
@@ -383,8 +391,8 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
                 if constexpr (FORCE) v[i] += a.c[k].force[i];
                 v[i] = stored_value<S>(v[i]);
             }
-            // the rest population closes the node's mass (sum_i d*_i = drho + sum_i F_i)
-            v[0] = mass_closing_rest(v, FORCE ? dr[k] + a.c[k].force_sum : dr[k]);
+            // the rest population closes the node's mass (sum_i d*_i = sum_i d_i + sum_i F_i)
+            v[0] = mass_closing_rest(f[k], v, FORCE ? a.c[k].force_sum : 0.f);
 #pragma unroll
             for (int i = 0; i < 9; ++i) {
                 float vi = v[i];
@@ -872,7 +880,7 @@ __global__ void __launch_bounds__(256) k_fused1(const Fused1Args<S, T> a)
                 v[i] = stored_value<S>(v[i]);
             }
             // the rest population closes the node's mass (see mass_closing_rest)
-            v[0] = mass_closing_rest(v, a.c.force_on ? dr + a.c.force_sum : dr);
+            v[0] = mass_closing_rest(f, v, a.c.force_on ? a.c.force_sum : 0.f);
 #pragma unroll
             for (int i = 0; i < 9; ++i) out[i] = v[i];
         }

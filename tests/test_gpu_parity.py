@@ -113,28 +113,30 @@ def density_errors(a, b, mask):
         float(np.linalg.norm(d) / np.linalg.norm(b[m]))
 
 
-# Tolerances: measured errors on a B200 times ~4.  FP32 rounding of the stored
-# deviations (~6e-8 |d_i| per step) accumulates over the run and is amplified by
-# the two-phase dynamics; spinodal decomposition at G = 1.2 amplifies a 1-ulp
-# FP64 perturbation 1e4-fold within 100 steps, so it is checked early (20
-# steps), before that growth dominates.
+# Tolerances: about twice the errors measured on a B200 (rho_ref = the mean
+# initial density of each component).  FP32 rounding of the stored deviations
+# (~6e-8 |d_i| per step) accumulates over the run; the rest population closes
+# each node's mass, so no systematic drift adds to it.  Spinodal decomposition
+# at G = 1.2 amplifies a 1-ulp FP64 perturbation 1e4-fold within 100 steps, so
+# it is checked early (20 steps), before that growth dominates.  L2 errors are
+# bounded by the max/mean errors, so they share the tolerance.
 SHIFTED_CASES = [
-    # name, steps, precision, max/mean tol, L2 tol
-    ("laplace_64x64", 150, "FP32_SHIFTED", 1e-4, 1e-5),
-    ("channel_80x32", 100, "FP32_SHIFTED", 1e-4, 1e-5),
-    ("porous_96x48", 120, "FP32_SHIFTED", 2e-4, 1e-5),
-    ("spinodal_48x40", 20, "FP32_SHIFTED", 5e-6, 1e-6),
-    ("poiseuille_200x50", 100, "FP32_SHIFTED", 1e-7, 1e-7),
-    ("laplace_64x64", 150, "FP16_SHIFTED", 0.15, 1e-2),
-    ("channel_80x32", 100, "FP16_SHIFTED", 0.05, 7e-3),
-    ("porous_96x48", 120, "FP16_SHIFTED", 0.15, 7e-3),
-    ("spinodal_48x40", 20, "FP16_SHIFTED", 5e-3, 1.2e-3),
-    ("poiseuille_200x50", 100, "FP16_SHIFTED", 1e-6, 1e-6),
+    # name, steps, precision, max/mean tol (measured)
+    ("laplace_64x64", 150, "FP32_SHIFTED", 3e-6),     # 1.4e-6
+    ("channel_80x32", 100, "FP32_SHIFTED", 4e-5),     # 2.1e-5
+    ("porous_96x48", 120, "FP32_SHIFTED", 1e-5),      # 5.4e-6
+    ("spinodal_48x40", 20, "FP32_SHIFTED", 4e-7),     # 1.9e-7
+    ("poiseuille_200x50", 100, "FP32_SHIFTED", 1e-7),
+    ("laplace_64x64", 150, "FP16_SHIFTED", 3.5e-2),   # 1.6e-2
+    ("channel_80x32", 100, "FP16_SHIFTED", 2e-2),     # 9.1e-3
+    ("porous_96x48", 120, "FP16_SHIFTED", 3e-2),      # 1.4e-2
+    ("spinodal_48x40", 20, "FP16_SHIFTED", 2.5e-3),   # 1.1e-3
+    ("poiseuille_200x50", 100, "FP16_SHIFTED", 1e-6),
 ]
 
 
-@pytest.mark.parametrize("name,steps,prec,tol_max,tol_l2", SHIFTED_CASES)
-def test_shifted_forms_density_error(sclbm, oracle, name, steps, prec, tol_max, tol_l2):
+@pytest.mark.parametrize("name,steps,prec,tol_max", SHIFTED_CASES)
+def test_shifted_forms_density_error(sclbm, oracle, name, steps, prec, tol_max):
     """Shifted storage (f_i - w_i*rho_ref, rho_ref = mean initial density) with
     FP32 arithmetic stays within the stated density error of the FP64 oracle."""
     case = dict(RUNS[name], steps=steps)
@@ -146,7 +148,41 @@ def test_shifted_forms_density_error(sclbm, oracle, name, steps, prec, tol_max, 
     got = gpu_runner.run_domain(sclbm, case, getattr(sclbm, prec), rho_ref=rr[:2])
     for c in ("c1_", "c2_") if case["mode"] == "two" else ("c1_",):
         e_max, e_l2 = density_errors(got[c + "rho_final"], want[c + "rho_final"], want["mask"])
-        assert e_max <= tol_max and e_l2 <= tol_l2, (name, prec, c, e_max, e_l2)
+        assert e_max <= tol_max and e_l2 <= tol_max, (name, prec, c, e_max, e_l2)
+
+
+@pytest.mark.parametrize("name,steps", [("laplace_64x64", 150), ("porous_96x48", 120)])
+def test_fp32_shifted_within_1e5_on_stable_two_phase(sclbm, oracle, name, steps):
+    """The north-star accuracy bar: FP32-shifted densities within 1e-5 of the
+    mean density of the FP64 oracle (bit-exact with the reference) on stable
+    two-phase states -- a droplet at rest, and two components with wetting
+    walls in a porous medium -- with each component's mean initial density as
+    rho_ref."""
+    case = dict(RUNS[name], steps=steps)
+    want = oracle.run_case(case)
+    N = case["nx"] * case["ny"]
+    m = want["mask"].astype(bool)
+    f0 = gpu_runner._init_f(case, want["mask"].astype(np.uint8))
+    rr = tuple(float(f.reshape(9, N).sum(0)[m].mean()) for f in f0)
+    got = gpu_runner.run_domain(sclbm, case, sclbm.FP32_SHIFTED, rho_ref=rr)
+    for c in ("c1_", "c2_"):
+        e_max, _ = density_errors(got[c + "rho_final"], want[c + "rho_final"], want["mask"])
+        assert e_max <= 1e-5, (name, c, e_max)
+
+
+def test_shifted_forms_close_each_nodes_mass(sclbm):
+    """The rest population closes every node's mass, so the shifted forms keep
+    the total mass of a droplet at rest (no systematic drift from the
+    float-rounded weights, whose sum is 1 + 7.5e-9: 2,000 steps of that bias
+    drifted ~1e-5 of the mass)."""
+    case = dict(RUNS["laplace_64x64"], steps=0)
+    for prec, tol in ((sclbm.FP32_SHIFTED, 1e-7), (sclbm.FP16_SHIFTED, 1e-2)):
+        d = gpu_runner.make_domain(sclbm, case, prec, rho_ref=(0.4, 1.1))
+        m0 = d.mass_momentum()
+        d.step(2000)
+        m1 = d.mass_momentum()
+        for k in range(2):
+            assert abs(m1[3 * k] - m0[3 * k]) <= tol * abs(m0[3 * k]), (prec, k, m1[3 * k] / m0[3 * k] - 1)
 
 
 @pytest.mark.parametrize("variant,tile_y,tx", [(1, 4, 128), (4, 0, 128), (4, 7, 128), (3, 0, 128),
@@ -216,8 +252,8 @@ def test_mass_momentum_monitor(sclbm):
 
 def test_mass_conserved_in_periodic_domain(sclbm):
     case = dict(RUNS["spinodal_48x40"], steps=0)
-    # FP32: measured 1.1e-6 over 500 steps (rounding of the stored deviations)
-    for prec, tol in ((sclbm.FP64, 1e-13), (sclbm.FP32_SHIFTED, 5e-6)):
+    # FP32: no systematic drift (the rest population closes each node's mass)
+    for prec, tol in ((sclbm.FP64, 1e-13), (sclbm.FP32_SHIFTED, 1e-7)):
         d = gpu_runner.make_domain(sclbm, case, prec)
         m0 = d.mass_momentum()
         d.step(500)

@@ -132,46 +132,71 @@ template <typename T, int FLAGS> constexpr int ring_min_ctas()
     return sizeof(T) == 8 ? 3 : ((FLAGS & KF_UNIFORM) ? 5 : 6);
 }
 
-// One band of one strip per CTA; band b covers rows [b*ny/bands, (b+1)*ny/bands).
+// The shared-memory pieces of one CTA's ring.
+template <typename S, typename T, int R> struct RingShared {
+    unsigned char *base; // 128-byte aligned: the R stages
+    V2<T> *rho;          // density ring [4][Q]
+    uint8_t *msk;        // mask ring [4][Q]
+    uint64_t *bars;      // one mbarrier per stage
+    volatile int *abort_flag;
+};
+
+template <typename S, typename T, int R>
+__device__ __forceinline__ RingShared<S, T, R> ring_shared(unsigned char *raw)
+{
+    using L = RingLayout<S, T, R>;
+    RingShared<S, T, R> sh;
+    sh.base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(raw) + 127) & ~uintptr_t(127));
+    sh.rho = reinterpret_cast<V2<T> *>(sh.base + L::pops);
+    sh.msk = sh.base + L::pops + L::rho;
+    sh.bars = reinterpret_cast<uint64_t *>(sh.base + L::bars);
+    sh.abort_flag = reinterpret_cast<volatile int *>(sh.base + L::bars + R * 8);
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < R; ++s) mbar_init(smem_addr(&sh.bars[s]), 1);
+        *sh.abort_flag = 0;
+        mbar_fence_init();
+    }
+    __syncthreads();
+    return sh;
+}
+
+// One unit of work: strip [xb, xb + RING_W) of rows [y0, y0 + nrow) of the
+// lattice of `a`, rows marched upward or (down) downward.  The ring rows of
+// a CTA are numbered on across its units (g0, advanced here), so every
+// stage's mbarrier phase follows from that count.  maps: row boxes of both
+// components, then halo boxes.  Returns false once the CTA has given up on a
+// bounded wait (*a.status is then set).
 template <typename S, typename T, int FLAGS, int R, bool WIDE>
-__global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS>()))
-    k_ring2(const __grid_constant__ Fused2Args<S, T> a, const __grid_constant__ RingMaps maps, int bands)
+__device__ __forceinline__ bool ring_unit(const Fused2Args<S, T> &a, const CUtensorMap *map_row0,
+                                          const CUtensorMap *map_row1, const CUtensorMap *map_halo0,
+                                          const CUtensorMap *map_halo1, const int xb, const int y0,
+                                          const int nrow, const bool down, const RingShared<S, T, R> &sh,
+                                          uint32_t &g0)
 {
     using L = RingLayout<S, T, R>;
     constexpr int A = L::A, P = L::P, Q = L::Q;
     constexpr uint32_t CE = L::CE;
     constexpr bool SOLID = (FLAGS & KF_SOLID) != 0;
-    extern __shared__ __align__(128) unsigned char ring_raw[];
-    unsigned char *ring_smem =
-        reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(ring_raw) + 127) & ~uintptr_t(127));
-    V2<T> *rho = reinterpret_cast<V2<T> *>(ring_smem + L::pops);
-    uint8_t *msk = ring_smem + L::pops + L::rho;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(ring_smem + L::bars);
-    volatile int *abort_flag = reinterpret_cast<volatile int *>(ring_smem + L::bars + R * 8);
+    unsigned char *const ring_smem = sh.base;
+    V2<T> *const rho = sh.rho;
+    uint8_t *const msk = sh.msk;
+    uint64_t *const bars = sh.bars;
+    volatile int *const abort_flag = sh.abort_flag;
 
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int nx = a.nx, ny = a.ny;
-    const int xb = blockIdx.x * RING_W;
     const int ncol = min(RING_W, nx - xb);
-    const int band = blockIdx.y;
-    const int y0 = (int)((long long)band * ny / bands);
-    const int nrow = (int)((long long)(band + 1) * ny / bands) - y0;
-    const bool down = (band & 1) != 0;
     const bool act = t < ncol;
     const bool hl = t == 0, hr = t == ncol - 1;
     const int x = act ? xb + t : xb;
     const int xl = wrap1(x - 1, nx), xr = wrap1(x + 1, nx);
     const int xhl = wrap1(xb - 1, nx), xhr = wrap1(xb + ncol, nx);
     const int last = nrow + 1;
+    const uint32_t gbase = g0;
     // lattice row of ring row j (tile row -1 .. nrow in march order)
     auto gy = [&](int j) { return wrap1(y0 + (down ? nrow - j : j - 1), ny); };
-
-    if (t == 0) {
-        for (int s = 0; s < R; ++s) mbar_init(smem_addr(&bars[s]), 1);
-        *abort_flag = 0;
-        mbar_fence_init();
-    }
-    __syncthreads();
+    auto stage_of = [&](int j) { return (int)((gbase + (uint32_t)j) % (uint32_t)R); };
+    auto phase_of = [&](int j) { return ((gbase + (uint32_t)j) / (uint32_t)R) & 1u; };
 
     // the halo column left (right) of the strip wraps around the lattice edge:
     // it comes from an A-column box at the other edge
@@ -183,41 +208,37 @@ __global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS>()))
     // lane 0 of warp 0 requests row j: one box per component (+ halo boxes)
     auto issue = [&](int j) {
         if (lane != 0) return;
-        const int st = j % R;
+        const int st = stage_of(j);
         const uint32_t bar = smem_addr(&bars[st]);
         const uint32_t sb = smem_addr(stage_at(st));
         const int y = gy(j);
         mbar_expect_tx(bar, row_bytes);
+        const CUtensorMap *rowm[2] = {map_row0, map_row1}, *halom[2] = {map_halo0, map_halo1};
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
-            tensor_g2s_3d(sb + k * (uint32_t)L::comp, &maps.row[k], xb - A, y, 0, bar);
+            tensor_g2s_3d(sb + k * (uint32_t)L::comp, rowm[k], xb - A, y, 0, bar);
             if (wrap_l)
-                tensor_g2s_3d(sb + 2 * (uint32_t)L::comp + (0 + k) * (uint32_t)L::halo, &maps.halo[k],
-                              nx - A, y, 0, bar);
+                tensor_g2s_3d(sb + 2 * (uint32_t)L::comp + (0 + k) * (uint32_t)L::halo, halom[k], nx - A, y,
+                              0, bar);
             if (wrap_r)
-                tensor_g2s_3d(sb + 2 * (uint32_t)L::comp + (2 + k) * (uint32_t)L::halo, &maps.halo[k], 0,
-                              y, 0, bar);
+                tensor_g2s_3d(sb + 2 * (uint32_t)L::comp + (2 + k) * (uint32_t)L::halo, halom[k], 0, y, 0,
+                              bar);
         }
     };
     auto wait_row = [&](int j) {
-        const uint32_t bar = smem_addr(&bars[j % R]);
-        const uint32_t par = (uint32_t)((j / R) & 1);
+        const uint32_t bar = smem_addr(&bars[stage_of(j)]);
+        const uint32_t par = phase_of(j);
         for (int it = 0; it < RING_WAIT_LIMIT; ++it)
             if (mbar_try_wait(bar, par)) return true;
         return false;
     };
 
     int issued = -1; // last row requested (warp 0's view)
-    if (warp == 0) {
-        if (lane == 0) {
-            asm volatile("prefetch.tensormap [%0];" ::"l"(&maps.row[0]) : "memory");
-            asm volatile("prefetch.tensormap [%0];" ::"l"(&maps.row[1]) : "memory");
-        }
+    if (warp == 0)
         for (int j = 0; j < R && j <= last; ++j) {
             issue(j);
             issued = j;
         }
-    }
 
     // masks of the next row, loaded one row ahead
     uint8_t mn = 1, mnl = 1, mnr = 1;
@@ -245,7 +266,7 @@ __global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS>()))
         if (!aborted) {
             if (wait_row(j)) {
                 consumed = j;
-                const unsigned char *sg = stage_at(j % R);
+                const unsigned char *sg = stage_at(stage_of(j));
                 const S *stg = reinterpret_cast<const S *>(sg);
                 const S *hlp = reinterpret_cast<const S *>(sg + 2 * L::comp);            // [k][9][A]
                 const S *hrp = reinterpret_cast<const S *>(sg + 2 * L::comp + 2 * L::halo);
@@ -325,6 +346,81 @@ __global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS>()))
         // let the copies still in flight land before the CTA's shared memory is released
         for (int j = consumed + 1; j <= issued; ++j) (void)wait_row(j);
     }
+    g0 = gbase + (uint32_t)(last + 1);
+    return !aborted;
+}
+
+// One band of one strip per CTA; band b covers rows [b*ny/bands, (b+1)*ny/bands).
+template <typename S, typename T, int FLAGS, int R, bool WIDE>
+__global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS>()))
+    k_ring2(const __grid_constant__ Fused2Args<S, T> a, const __grid_constant__ RingMaps maps, int bands)
+{
+    extern __shared__ __align__(128) unsigned char ring_raw[];
+    const RingShared<S, T, R> sh = ring_shared<S, T, R>(ring_raw);
+    if (threadIdx.x == 0) {
+        asm volatile("prefetch.tensormap [%0];" ::"l"(&maps.row[0]) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(&maps.row[1]) : "memory");
+    }
+    const int band = blockIdx.y;
+    const int y0 = (int)((long long)band * a.ny / bands);
+    const int nrow = (int)((long long)(band + 1) * a.ny / bands) - y0;
+    uint32_t g = 0;
+    (void)ring_unit<S, T, FLAGS, R, WIDE>(a, &maps.row[0], &maps.row[1], &maps.halo[0], &maps.halo[1],
+                                          blockIdx.x * RING_W, y0, nrow, (band & 1) != 0, sh, g);
+}
+
+// A unit of the batched ring kernel: strip xb of rows [y0, y1) of domain dom;
+// down: the march direction (alternating between a domain's bands).
+struct RingUnit {
+    int dom, xb, y0, y1, down, pad[3];
+};
+
+// Batched ring kernel: every CTA takes units from a shared counter (largest
+// units first in the list) until the list is exhausted; the last CTA to finish
+// resets the counters for the next launch (kernel boundaries order it).  No
+// CTA waits on another.  doms and maps hold two entries per domain (buffer
+// parity 0 and 1); the current unit's argument block is copied into shared
+// memory.  counters: [0] the next unit, [1] CTAs finished.
+template <typename S, typename T, int FLAGS, int R>
+__global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS>()))
+    k_batch_ring(const Fused2Args<S, T> *__restrict__ doms, const RingMaps *__restrict__ maps,
+                 const RingUnit *__restrict__ units, int nunits, int parity, unsigned *counters)
+{
+    extern __shared__ __align__(128) unsigned char ring_raw[];
+    __shared__ __align__(16) Fused2Args<S, T> sa;
+    __shared__ int s_next;
+    static_assert(sizeof(Fused2Args<S, T>) % 4 == 0, "argument block copied as words");
+    const RingShared<S, T, R> sh = ring_shared<S, T, R>(ring_raw);
+    uint32_t g = 0;
+    int loaded = -1;
+    for (;;) {
+        if (threadIdx.x == 0) s_next = (int)atomicAdd(&counters[0], 1u);
+        __syncthreads();
+        const int i = s_next;
+        if (i >= nunits) break;
+        const RingUnit u = units[i];
+        const int key = 2 * u.dom + parity;
+        if (key != loaded) { // uniform over the CTA
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(doms + key);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(&sa);
+            for (int w = threadIdx.x; w < (int)(sizeof(sa) / 4); w += RING_W) dst[w] = src[w];
+            __syncthreads();
+            loaded = key;
+        }
+        const RingMaps *m = maps + key;
+        const bool ok = ring_unit<S, T, FLAGS, R, false>(sa, &m->row[0], &m->row[1], &m->halo[0],
+                                                          &m->halo[1], u.xb, u.y0, u.y1 - u.y0,
+                                                          u.down != 0, sh, g);
+        __syncthreads(); // the ring, s_next and the argument block are reused by the next unit
+        if (!ok) break;
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&counters[1], 1u) == gridDim.x - 1) { // the last CTA out
+            counters[0] = 0;
+            counters[1] = 0;
+        }
+    }
 }
 
 // tensor maps of the input populations of both components (host)
@@ -390,6 +486,49 @@ inline cudaError_t launch_ring2_any(const Fused2Args<S, T> &a, cudaStream_t s)
     case KF_SOLID: return launch_ring2_f<S, T, KF_SOLID | UNI, R, false>(a, s);
     default: return launch_ring2_f<S, T, KF_FORCE | KF_SOLID | UNI, R, false>(a, s);
     }
+}
+
+// ---------------------------------------------------------------- batches
+// UNI: the uniform solid form for batches holding solid nodes (FP32/FP16)
+template <typename S, typename T, int R, int UNI, int FLAGS>
+inline cudaError_t batch_ring_prepare_f(int *per_sm)
+{
+    using L = RingLayout<S, T, R>;
+    auto kern = k_batch_ring<S, T, FLAGS, R>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes);
+    if (e != cudaSuccess) return e;
+    int n = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, RING_W, L::bytes);
+    if (per_sm) *per_sm = n;
+    return e;
+}
+
+// sets the shared-memory limit of every body the batch may run (outside any
+// graph capture) and returns the resident CTAs per SM of the solid body
+template <typename S, typename T, int R, int UNI>
+inline cudaError_t batch_ring_prepare(int *per_sm)
+{
+    cudaError_t e = batch_ring_prepare_f<S, T, R, UNI, 0>(nullptr);
+    if (e == cudaSuccess) e = batch_ring_prepare_f<S, T, R, UNI, KF_FORCE>(nullptr);
+    if (e == cudaSuccess) e = batch_ring_prepare_f<S, T, R, UNI, KF_FORCE | KF_SOLID | UNI>(per_sm);
+    return e;
+}
+
+template <typename S, typename T, int R, int UNI>
+inline cudaError_t launch_batch_ring(const Fused2Args<S, T> *doms, const RingMaps *maps,
+                                     const RingUnit *units, int nunits, int parity, int grid, int flags,
+                                     unsigned *counters, cudaStream_t s)
+{
+    using L = RingLayout<S, T, R>;
+    if (flags & KF_SOLID)
+        k_batch_ring<S, T, KF_FORCE | KF_SOLID | UNI, R><<<grid, RING_W, L::bytes, s>>>(
+            doms, maps, units, nunits, parity, counters);
+    else if (flags == KF_FORCE)
+        k_batch_ring<S, T, KF_FORCE, R><<<grid, RING_W, L::bytes, s>>>(doms, maps, units, nunits, parity,
+                                                                        counters);
+    else
+        k_batch_ring<S, T, 0, R><<<grid, RING_W, L::bytes, s>>>(doms, maps, units, nunits, parity, counters);
+    return cudaGetLastError();
 }
 
 } // namespace sclbm

@@ -138,6 +138,26 @@ cudaError_t launch_batch2_async_f32(const Fused2Args<float, float> *doms, const 
 cudaError_t launch_ring2_fp64(const Fused2Args<double, double> &a, int stages, cudaStream_t s);
 cudaError_t launch_ring2_f32(const Fused2Args<float, float> &a, int stages, cudaStream_t s);
 cudaError_t launch_ring2_f16(const Fused2Args<__half, float> &a, int stages, cudaStream_t s);
+// batched ring kernel (fused_ring.cuh): maps and units are device arrays
+// (RingMaps per domain and parity; RingUnit work list); counters: two
+// device words, zero before the first launch
+struct RingMaps;
+struct RingUnit;
+cudaError_t launch_batch_ring_fp64(const Fused2Args<double, double> *doms, const RingMaps *maps,
+                                   const RingUnit *units, int nunits, int parity, int grid, int flags,
+                                   unsigned *counters, cudaStream_t s);
+cudaError_t launch_batch_ring_f32(const Fused2Args<float, float> *doms, const RingMaps *maps,
+                                  const RingUnit *units, int nunits, int parity, int grid, int flags,
+                                  unsigned *counters, cudaStream_t s);
+cudaError_t launch_batch_ring_f16(const Fused2Args<__half, float> *doms, const RingMaps *maps,
+                                  const RingUnit *units, int nunits, int parity, int grid, int flags,
+                                  unsigned *counters, cudaStream_t s);
+// shared-memory limits and resident CTAs per SM of the batched ring kernel
+int batch_ring_prepare(sclbm_precision p, int *per_sm);
+// tensor maps of a domain's argument block (host); 0 on success
+int ring_maps_of(const Fused2Args<double, double> &a, RingMaps *m);
+int ring_maps_of(const Fused2Args<float, float> &a, RingMaps *m);
+int ring_maps_of(const Fused2Args<__half, float> &a, RingMaps *m);
 int async_resident_fp64(); // CTAs of the batched kernel resident on the device
 int async_resident_f32();
 constexpr int ASYNC_STRIP = 128;

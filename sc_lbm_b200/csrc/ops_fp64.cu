@@ -444,4 +444,23 @@ cudaError_t launch_ring2_fp64(const Fused2Args<double, double> &a, int stages, c
     if (stages > 0) return launch_ring2_any<double, double, 4, 0>(a, s);
     return launch_ring2_any<double, double, 3, 0>(a, s);
 }
+constexpr int RING_BATCH_R64 = 3;
+cudaError_t launch_batch_ring_fp64(const Fused2Args<double, double> *doms, const RingMaps *maps,
+                                   const RingUnit *units, int nunits, int parity, int grid, int flags,
+                                   unsigned *counters, cudaStream_t s)
+{
+    return launch_batch_ring<double, double, RING_BATCH_R64, 0>(doms, maps, units, nunits, parity, grid,
+                                                                 flags, counters, s);
+}
+int batch_ring_prepare_shifted(sclbm_precision p, int *per_sm);
+int batch_ring_prepare(sclbm_precision p, int *per_sm)
+{
+    if (p != SCLBM_FP64) return batch_ring_prepare_shifted(p, per_sm);
+    const cudaError_t e = batch_ring_prepare<double, double, RING_BATCH_R64, 0>(per_sm);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "ring batch set-up");
+}
+int ring_maps_of(const Fused2Args<double, double> &a, RingMaps *m)
+{
+    return ring_maps<double, double, RING_BATCH_R64>(a, *m) == cudaSuccess ? 0 : 1;
+}
 } // namespace sclbm

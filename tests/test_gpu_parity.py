@@ -284,7 +284,9 @@ def test_batch_matches_individual_domains(sclbm):
                                 (sclbm.FP16_SHIFTED, False, 6), (sclbm.FP32_SHIFTED, True, 8),
                                 (sclbm.FP16_SHIFTED, True, 8), (sclbm.FP32_SHIFTED, True, 9),
                                 (sclbm.FP16_SHIFTED, False, 9), (sclbm.FP32_SHIFTED, True, 10),
-                                (sclbm.FP16_SHIFTED, False, 10)):
+                                (sclbm.FP16_SHIFTED, False, 10), (sclbm.FP32_SHIFTED, True, 11),
+                                (sclbm.FP16_SHIFTED, True, 11), (sclbm.FP64, True, 11),
+                                (sclbm.FP32_SHIFTED, False, 11)):
         rr = (0.8, 1.2)
         solo = [gpu_runner.run_domain(sclbm, dict(RUNS[n], steps=45), prec, rho_ref=rr) for n in names]
         doms = [gpu_runner.make_domain(sclbm, RUNS[n], prec, rho_ref=rr) for n in names]
@@ -296,7 +298,8 @@ def test_batch_matches_individual_domains(sclbm):
                 assert d.download_f(k).tobytes() == s[f"c{k + 1}_f"].tobytes(), (prec, n, k)
 
 
-def test_batch_fp64_matches_reference(sclbm):
+@pytest.mark.parametrize("kernel", [0, 11])
+def test_batch_fp64_matches_reference(sclbm, kernel):
     names = ["porous_96x48", "spinodal_48x40", "laplace_64x64"]
     doms = [gpu_runner.make_domain(sclbm, RUNS[n], sclbm.FP64) for n in names]
     steps = {RUNS[n]["steps"] for n in names}
@@ -305,11 +308,28 @@ def test_batch_fp64_matches_reference(sclbm):
         doms_by.setdefault(RUNS[n]["steps"], []).append((n, d))
     for st, group in doms_by.items():
         b = sclbm.Batch([d for _, d in group])
+        b.set_kernel(kernel)
         b.step(st, use_graph=True)
         for n, d in group:
             res = {"c1_f": d.download_f(0), "c2_f": d.download_f(1)}
             assert_golden(n, res, ["c1_f", "c2_f"])
+            d.mass_momentum()  # raises if a bounded wait ran out
     assert steps
+
+
+def test_batch_ring_needs_aligned_rows(sclbm):
+    """The ring body copies rows that start on 16-byte boundaries: a batch
+    holding a domain 130 wide refuses it in FP32 (130 is not a multiple of 4)
+    and keeps its other bodies."""
+    f = cases.noisy_f_equilibrium(3, 130, 6, 1.0, 0.02, 0.03)
+    case = dict(nx=130, ny=6, geom=[], mode="two", fluid1=(1.0, 1.0, 0.0), fluid2=(1.0, 1.0, 0.0),
+                init=("file", np.concatenate([f, f])), steps=3)
+    d = gpu_runner.make_domain(sclbm, case, sclbm.FP32_SHIFTED)
+    b = sclbm.Batch([d, gpu_runner.make_domain(sclbm, RUNS["spinodal_48x40"], sclbm.FP32_SHIFTED)])
+    with pytest.raises(ValueError):
+        b.set_kernel(11)
+    b.set_kernel(2)
+    b.step(3)
 
 
 # ----------------------------------------------------------------- error paths

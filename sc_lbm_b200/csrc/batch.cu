@@ -353,7 +353,7 @@ int sclbm_batch_set_kernel(sclbm_batch *b, int variant)
                          "16 bytes of storage (nx a multiple of 2, 4 or 8 for FP64, FP32, FP16)");
     if (variant == 3 && b->prec == SCLBM_FP16_SHIFTED)
         return set_error(SCLBM_E_INVALID_ARGUMENT, "the FP16 form uses the tile list (variant 2)");
-    if ((variant == 5 || variant == 6 || variant >= 8) && b->prec == SCLBM_FP64)
+    if ((variant == 5 || variant == 6 || (variant >= 8 && variant <= 10)) && b->prec == SCLBM_FP64)
         return set_error(SCLBM_E_INVALID_ARGUMENT,
                          "the load-ahead, compacted and uniform tile lists are for FP32/FP16 storage");
     b->use_ring = variant == 11;

@@ -47,15 +47,15 @@ struct sclbm_batch {
     int flags = 0;                 // KF_FORCE / KF_SOLID if any domain needs them
     cudaGraphExec_t graph[2] = {nullptr, nullptr}; // by starting parity
     cudaStream_t graph_stream = nullptr;
-    // ring body (variant 11): units of (domain, strip, band), tensor maps per
-    // domain and parity, the work counters; absent when a domain's rows do
-    // not start on 16-byte boundaries
+    // ring bodies (variant 11: 128-column strips, 12: 64-column strips): units
+    // of (domain, strip, band), tensor maps per domain and parity, the work
+    // counters; absent when a domain's rows do not start on 16-byte boundaries
     bool ring = false;
-    bool use_ring = false;
-    RingUnit *d_units = nullptr;
-    RingMaps *d_maps = nullptr;
+    int use_ring = 0; // 0, or the strip width of the ring body in use
+    RingUnit *d_units[2] = {nullptr, nullptr}; // [0] 128 wide, [1] 64 wide
+    RingMaps *d_maps[2] = {nullptr, nullptr};
     unsigned *d_counters = nullptr;
-    int nunits = 0, ring_grid = 0;
+    int nunits[2] = {0, 0}, ring_grid[2] = {0, 0};
 };
 
 // the tile list of the current body
@@ -71,19 +71,20 @@ static int batch_ntiles(const sclbm_batch *b)
 static cudaError_t batch_launch_any(sclbm_batch *b, int parity, cudaStream_t s)
 {
     if (b->use_ring) {
+        const int w = b->use_ring, r = w == 64 ? 1 : 0;
         switch (b->prec) {
         case SCLBM_FP64:
-            return launch_batch_ring_fp64((const Fused2Args<double, double> *)b->d_args, b->d_maps,
-                                          b->d_units, b->nunits, parity, b->ring_grid, b->flags,
-                                          b->d_counters, s);
+            return launch_batch_ring_fp64((const Fused2Args<double, double> *)b->d_args, b->d_maps[r],
+                                          b->d_units[r], b->nunits[r], parity, b->ring_grid[r], b->flags,
+                                          b->d_counters, w, s);
         case SCLBM_FP32_SHIFTED:
-            return launch_batch_ring_f32((const Fused2Args<float, float> *)b->d_args, b->d_maps,
-                                         b->d_units, b->nunits, parity, b->ring_grid, b->flags,
-                                         b->d_counters, s);
+            return launch_batch_ring_f32((const Fused2Args<float, float> *)b->d_args, b->d_maps[r],
+                                         b->d_units[r], b->nunits[r], parity, b->ring_grid[r], b->flags,
+                                         b->d_counters, w, s);
         default:
-            return launch_batch_ring_f16((const Fused2Args<__half, float> *)b->d_args, b->d_maps,
-                                         b->d_units, b->nunits, parity, b->ring_grid, b->flags,
-                                         b->d_counters, s);
+            return launch_batch_ring_f16((const Fused2Args<__half, float> *)b->d_args, b->d_maps[r],
+                                         b->d_units[r], b->nunits[r], parity, b->ring_grid[r], b->flags,
+                                         b->d_counters, w, s);
         }
     }
     if (b->use_units && b->prec == SCLBM_FP64)
@@ -105,15 +106,13 @@ static cudaError_t batch_launch_any(sclbm_batch *b, int parity, cudaStream_t s)
     }
 }
 
-// Ring body: every domain cut into 128-column strips and bands of about
-// `rows` rows (a domain's bands alternate their march direction), largest
-// units first; tensor maps of both parities of every domain.
+// Ring bodies: every domain cut into strips `width` columns wide and bands of
+// about `rows` rows (a domain's bands alternate their march direction),
+// largest units first; tensor maps of both parities of every domain.
 template <typename S, typename T>
-static int build_ring(sclbm_batch *b, const std::vector<Fused2Args<S, T>> &h, int rows)
+static int build_ring(sclbm_batch *b, const std::vector<Fused2Args<S, T>> &h, int rows, int width)
 {
-    const int A = 16 / (int)sizeof(S);
-    for (auto *d : b->doms)
-        if (d->nx % A != 0) return SCLBM_OK; // no ring body for this batch
+    const int r = width == 64 ? 1 : 0;
     std::vector<RingUnit> units;
     std::vector<long> cost;
     for (int k = 0; k < (int)b->doms.size(); ++k) {
@@ -121,9 +120,9 @@ static int build_ring(sclbm_batch *b, const std::vector<Fused2Args<S, T>> &h, in
         const int nb = std::max(1, (int)((d->ny + rows / 2) / rows));
         for (int j = 0; j < nb; ++j) {
             const int y0 = (int)((long long)d->ny * j / nb), y1 = (int)((long long)d->ny * (j + 1) / nb);
-            for (int xb = 0; xb < (int)d->nx; xb += RING_W) {
+            for (int xb = 0; xb < (int)d->nx; xb += width) {
                 units.push_back(RingUnit{k, xb, y0, y1, j & 1, {0, 0, 0}});
-                cost.push_back((long)std::min(RING_W, (int)d->nx - xb) * (y1 - y0 + 2));
+                cost.push_back((long)std::min(width, (int)d->nx - xb) * (y1 - y0 + 2));
             }
         }
     }
@@ -134,16 +133,29 @@ static int build_ring(sclbm_batch *b, const std::vector<Fused2Args<S, T>> &h, in
     for (size_t i = 0; i < order.size(); ++i) sorted[i] = units[order[i]];
     std::vector<RingMaps> maps(h.size());
     for (size_t i = 0; i < h.size(); ++i)
-        if (ring_maps_of(h[i], &maps[i])) return set_error(SCLBM_E_CUDA, "tensor map encoding");
+        if (ring_maps_of(h[i], width, &maps[i])) return set_error(SCLBM_E_CUDA, "tensor map encoding");
     int per_sm = 0;
-    int rc = batch_ring_prepare(b->prec, &per_sm);
+    int rc = batch_ring_prepare(b->prec, width, &per_sm);
     if (rc) return rc;
-    b->nunits = (int)sorted.size();
-    b->ring_grid = std::max(1, std::min(b->nunits, std::max(1, per_sm) * sm_count()));
-    SCLBM_CUDA(cudaMalloc(&b->d_units, sorted.size() * sizeof(RingUnit)));
-    SCLBM_CUDA(cudaMemcpy(b->d_units, sorted.data(), sorted.size() * sizeof(RingUnit), cudaMemcpyHostToDevice));
-    SCLBM_CUDA(cudaMalloc(&b->d_maps, maps.size() * sizeof(RingMaps)));
-    SCLBM_CUDA(cudaMemcpy(b->d_maps, maps.data(), maps.size() * sizeof(RingMaps), cudaMemcpyHostToDevice));
+    b->nunits[r] = (int)sorted.size();
+    b->ring_grid[r] = std::max(1, std::min(b->nunits[r], std::max(1, per_sm) * sm_count()));
+    SCLBM_CUDA(cudaMalloc(&b->d_units[r], sorted.size() * sizeof(RingUnit)));
+    SCLBM_CUDA(cudaMemcpy(b->d_units[r], sorted.data(), sorted.size() * sizeof(RingUnit),
+                          cudaMemcpyHostToDevice));
+    SCLBM_CUDA(cudaMalloc(&b->d_maps[r], maps.size() * sizeof(RingMaps)));
+    SCLBM_CUDA(cudaMemcpy(b->d_maps[r], maps.data(), maps.size() * sizeof(RingMaps), cudaMemcpyHostToDevice));
+    return SCLBM_OK;
+}
+
+template <typename S, typename T>
+static int build_rings(sclbm_batch *b, const std::vector<Fused2Args<S, T>> &h, int rows)
+{
+    const int A = 16 / (int)sizeof(S);
+    for (auto *d : b->doms)
+        if (d->nx % A != 0) return SCLBM_OK; // no ring body for this batch
+    int rc = build_ring<S, T>(b, h, rows, 128);
+    if (!rc) rc = build_ring<S, T>(b, h, rows, 64);
+    if (rc) return rc;
     SCLBM_CUDA(cudaMalloc(&b->d_counters, 2 * sizeof(unsigned)));
     SCLBM_CUDA(cudaMemset(b->d_counters, 0, 2 * sizeof(unsigned)));
     b->ring = true;
@@ -177,7 +189,7 @@ static int upload_args(sclbm_batch *b, const std::vector<int> &ty)
     SCLBM_CUDA(cudaMalloc(&b->d_args, h.size() * sizeof(Fused2Args<S, T>)));
     SCLBM_CUDA(cudaMemcpy(b->d_args, h.data(), h.size() * sizeof(Fused2Args<S, T>),
                           cudaMemcpyHostToDevice));
-    return build_ring<S, T>(b, h, RING_BATCH_ROWS);
+    return build_rings<S, T>(b, h, RING_BATCH_ROWS);
 }
 
 extern "C" {
@@ -192,8 +204,10 @@ void sclbm_batch_destroy(sclbm_batch *b)
     if (b->d_tiles_half) cudaFree(b->d_tiles_half);
     if (b->d_tiles_warp) cudaFree(b->d_tiles_warp);
     if (b->d_bands) cudaFree(b->d_bands);
-    if (b->d_units) cudaFree(b->d_units);
-    if (b->d_maps) cudaFree(b->d_maps);
+    for (int r = 0; r < 2; ++r) {
+        if (b->d_units[r]) cudaFree(b->d_units[r]);
+        if (b->d_maps[r]) cudaFree(b->d_maps[r]);
+    }
     if (b->d_counters) cudaFree(b->d_counters);
     delete b;
 }
@@ -345,9 +359,9 @@ int sclbm_batch_set_kernel(sclbm_batch *b, int variant)
 {
     if (!b) return set_error(SCLBM_E_INVALID_ARGUMENT, "null batch");
     if (variant != 0 && variant != 2 && variant != 3 && variant != 5 && variant != 6 && variant != 8 &&
-        variant != 9 && variant != 10 && variant != 11)
-        return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0, 2, 3, 5, 6, 8, 9, 10 or 11");
-    if (variant == 11 && !b->ring)
+        variant != 9 && variant != 10 && variant != 11 && variant != 12)
+        return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0, 2, 3, 5, 6, 8, 9, 10, 11 or 12");
+    if ((variant == 11 || variant == 12) && !b->ring)
         return set_error(SCLBM_E_INVALID_ARGUMENT,
                          "the ring body needs every domain's width to be a multiple of "
                          "16 bytes of storage (nx a multiple of 2, 4 or 8 for FP64, FP32, FP16)");
@@ -356,7 +370,7 @@ int sclbm_batch_set_kernel(sclbm_batch *b, int variant)
     if ((variant == 5 || variant == 6 || (variant >= 8 && variant <= 10)) && b->prec == SCLBM_FP64)
         return set_error(SCLBM_E_INVALID_ARGUMENT,
                          "the load-ahead, compacted and uniform tile lists are for FP32/FP16 storage");
-    b->use_ring = variant == 11;
+    b->use_ring = variant == 11 ? 128 : (variant == 12 ? 64 : 0);
     b->use_units = variant == 3 || (variant == 0 && b->auto_units);
     b->body = variant == 5   ? BODY_AHEAD
               : variant == 6 ? BODY_COMPACT
@@ -376,9 +390,10 @@ int sclbm_batch_set_kernel(sclbm_batch *b, int variant)
 int sclbm_batch_info(const sclbm_batch *b, int *ntiles, int *grid_ctas)
 {
     if (!b) return set_error(SCLBM_E_INVALID_ARGUMENT, "null batch");
-    if (ntiles) *ntiles = b->use_ring ? b->nunits : (b->use_units ? b->ntiles : batch_ntiles(b));
+    const int r = b->use_ring == 64 ? 1 : 0;
+    if (ntiles) *ntiles = b->use_ring ? b->nunits[r] : (b->use_units ? b->ntiles : batch_ntiles(b));
     if (grid_ctas)
-        *grid_ctas = b->use_ring    ? b->ring_grid
+        *grid_ctas = b->use_ring    ? b->ring_grid[r]
                      : b->use_units ? b->band_grid
                                     : (b->prec == SCLBM_FP64 ? b->grid : b->grid_body[b->body]);
     return SCLBM_OK;

@@ -52,10 +52,10 @@ constexpr int RING_WAIT_LIMIT = 1 << 20; // polls of one stage before giving up 
 // elements per 16 bytes of storage type S
 template <typename S> constexpr int ring_pad() { return 16 / (int)sizeof(S); }
 
-template <typename S, typename T, int R> struct RingLayout {
+template <typename S, typename T, int R, int W = RING_W> struct RingLayout {
     static constexpr int A = ring_pad<S>();
-    static constexpr int P = RING_W + 2 * A; // box columns
-    static constexpr int Q = RING_W + 2;     // density ring columns
+    static constexpr int P = W + 2 * A; // box columns
+    static constexpr int Q = W + 2;     // density ring columns
     // tensor-copy destinations start on 128-byte boundaries
     static constexpr size_t comp = (size_t(9) * P * sizeof(S) + 127) & ~size_t(127);
     static constexpr size_t halo = 256; // one A-column box of one component (144 bytes)
@@ -133,7 +133,7 @@ template <typename T, int FLAGS> constexpr int ring_min_ctas()
 }
 
 // The shared-memory pieces of one CTA's ring.
-template <typename S, typename T, int R> struct RingShared {
+template <typename S, typename T, int R, int W = RING_W> struct RingShared {
     unsigned char *base; // 128-byte aligned: the R stages
     V2<T> *rho;          // density ring [4][Q]
     uint8_t *msk;        // mask ring [4][Q]
@@ -141,11 +141,11 @@ template <typename S, typename T, int R> struct RingShared {
     volatile int *abort_flag;
 };
 
-template <typename S, typename T, int R>
-__device__ __forceinline__ RingShared<S, T, R> ring_shared(unsigned char *raw)
+template <typename S, typename T, int R, int W = RING_W>
+__device__ __forceinline__ RingShared<S, T, R, W> ring_shared(unsigned char *raw)
 {
-    using L = RingLayout<S, T, R>;
-    RingShared<S, T, R> sh;
+    using L = RingLayout<S, T, R, W>;
+    RingShared<S, T, R, W> sh;
     sh.base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(raw) + 127) & ~uintptr_t(127));
     sh.rho = reinterpret_cast<V2<T> *>(sh.base + L::pops);
     sh.msk = sh.base + L::pops + L::rho;
@@ -166,14 +166,14 @@ __device__ __forceinline__ RingShared<S, T, R> ring_shared(unsigned char *raw)
 // stage's mbarrier phase follows from that count.  maps: row boxes of both
 // components, then halo boxes.  Returns false once the CTA has given up on a
 // bounded wait (*a.status is then set).
-template <typename S, typename T, int FLAGS, int R, bool WIDE>
+template <typename S, typename T, int FLAGS, int R, bool WIDE, int W = RING_W>
 __device__ __forceinline__ bool ring_unit(const Fused2Args<S, T> &a, const CUtensorMap *map_row0,
                                           const CUtensorMap *map_row1, const CUtensorMap *map_halo0,
                                           const CUtensorMap *map_halo1, const int xb, const int y0,
-                                          const int nrow, const bool down, const RingShared<S, T, R> &sh,
+                                          const int nrow, const bool down, const RingShared<S, T, R, W> &sh,
                                           uint32_t &g0)
 {
-    using L = RingLayout<S, T, R>;
+    using L = RingLayout<S, T, R, W>;
     constexpr int A = L::A, P = L::P, Q = L::Q;
     constexpr uint32_t CE = L::CE;
     constexpr bool SOLID = (FLAGS & KF_SOLID) != 0;
@@ -185,7 +185,7 @@ __device__ __forceinline__ bool ring_unit(const Fused2Args<S, T> &a, const CUten
 
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int nx = a.nx, ny = a.ny;
-    const int ncol = min(RING_W, nx - xb);
+    const int ncol = min(W, nx - xb);
     const bool act = t < ncol;
     const bool hl = t == 0, hr = t == ncol - 1;
     const int x = act ? xb + t : xb;
@@ -381,8 +381,8 @@ struct RingUnit {
 // CTA waits on another.  doms and maps hold two entries per domain (buffer
 // parity 0 and 1); the current unit's argument block is copied into shared
 // memory.  counters: [0] the next unit, [1] CTAs finished.
-template <typename S, typename T, int FLAGS, int R>
-__global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS>()))
+template <typename S, typename T, int FLAGS, int R, int W>
+__global__ void __launch_bounds__(W, (ring_min_ctas<T, FLAGS>() * (RING_W / W)))
     k_batch_ring(const Fused2Args<S, T> *__restrict__ doms, const RingMaps *__restrict__ maps,
                  const RingUnit *__restrict__ units, int nunits, int parity, unsigned *counters)
 {
@@ -390,7 +390,7 @@ __global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS>()))
     __shared__ __align__(16) Fused2Args<S, T> sa;
     __shared__ int s_next;
     static_assert(sizeof(Fused2Args<S, T>) % 4 == 0, "argument block copied as words");
-    const RingShared<S, T, R> sh = ring_shared<S, T, R>(ring_raw);
+    const RingShared<S, T, R, W> sh = ring_shared<S, T, R, W>(ring_raw);
     uint32_t g = 0;
     int loaded = -1;
     for (;;) {
@@ -403,12 +403,12 @@ __global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS>()))
         if (key != loaded) { // uniform over the CTA
             const uint32_t *src = reinterpret_cast<const uint32_t *>(doms + key);
             uint32_t *dst = reinterpret_cast<uint32_t *>(&sa);
-            for (int w = threadIdx.x; w < (int)(sizeof(sa) / 4); w += RING_W) dst[w] = src[w];
+            for (int w = threadIdx.x; w < (int)(sizeof(sa) / 4); w += W) dst[w] = src[w];
             __syncthreads();
             loaded = key;
         }
         const RingMaps *m = maps + key;
-        const bool ok = ring_unit<S, T, FLAGS, R, false>(sa, &m->row[0], &m->row[1], &m->halo[0],
+        const bool ok = ring_unit<S, T, FLAGS, R, false, W>(sa, &m->row[0], &m->row[1], &m->halo[0],
                                                           &m->halo[1], u.xb, u.y0, u.y1 - u.y0,
                                                           u.down != 0, sh, g);
         __syncthreads(); // the ring, s_next and the argument block are reused by the next unit
@@ -424,10 +424,10 @@ __global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS>()))
 }
 
 // tensor maps of the input populations of both components (host)
-template <typename S, typename T, int R>
+template <typename S, typename T, int R, int W = RING_W>
 inline cudaError_t ring_maps(const Fused2Args<S, T> &a, RingMaps &m)
 {
-    using L = RingLayout<S, T, R>;
+    using L = RingLayout<S, T, R, W>;
     const CUtensorMapDataType dt = sizeof(S) == 8   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
                                    : sizeof(S) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                                     : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
@@ -490,44 +490,44 @@ inline cudaError_t launch_ring2_any(const Fused2Args<S, T> &a, cudaStream_t s)
 
 // ---------------------------------------------------------------- batches
 // UNI: the uniform solid form for batches holding solid nodes (FP32/FP16)
-template <typename S, typename T, int R, int UNI, int FLAGS>
+template <typename S, typename T, int R, int UNI, int FLAGS, int W>
 inline cudaError_t batch_ring_prepare_f(int *per_sm)
 {
-    using L = RingLayout<S, T, R>;
-    auto kern = k_batch_ring<S, T, FLAGS, R>;
+    using L = RingLayout<S, T, R, W>;
+    auto kern = k_batch_ring<S, T, FLAGS, R, W>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes);
     if (e != cudaSuccess) return e;
     int n = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, RING_W, L::bytes);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, W, L::bytes);
     if (per_sm) *per_sm = n;
     return e;
 }
 
 // sets the shared-memory limit of every body the batch may run (outside any
 // graph capture) and returns the resident CTAs per SM of the solid body
-template <typename S, typename T, int R, int UNI>
+template <typename S, typename T, int R, int UNI, int W>
 inline cudaError_t batch_ring_prepare(int *per_sm)
 {
-    cudaError_t e = batch_ring_prepare_f<S, T, R, UNI, 0>(nullptr);
-    if (e == cudaSuccess) e = batch_ring_prepare_f<S, T, R, UNI, KF_FORCE>(nullptr);
-    if (e == cudaSuccess) e = batch_ring_prepare_f<S, T, R, UNI, KF_FORCE | KF_SOLID | UNI>(per_sm);
+    cudaError_t e = batch_ring_prepare_f<S, T, R, UNI, 0, W>(nullptr);
+    if (e == cudaSuccess) e = batch_ring_prepare_f<S, T, R, UNI, KF_FORCE, W>(nullptr);
+    if (e == cudaSuccess) e = batch_ring_prepare_f<S, T, R, UNI, KF_FORCE | KF_SOLID | UNI, W>(per_sm);
     return e;
 }
 
-template <typename S, typename T, int R, int UNI>
+template <typename S, typename T, int R, int UNI, int W>
 inline cudaError_t launch_batch_ring(const Fused2Args<S, T> *doms, const RingMaps *maps,
                                      const RingUnit *units, int nunits, int parity, int grid, int flags,
                                      unsigned *counters, cudaStream_t s)
 {
-    using L = RingLayout<S, T, R>;
+    using L = RingLayout<S, T, R, W>;
     if (flags & KF_SOLID)
-        k_batch_ring<S, T, KF_FORCE | KF_SOLID | UNI, R><<<grid, RING_W, L::bytes, s>>>(
+        k_batch_ring<S, T, KF_FORCE | KF_SOLID | UNI, R, W><<<grid, W, L::bytes, s>>>(
             doms, maps, units, nunits, parity, counters);
     else if (flags == KF_FORCE)
-        k_batch_ring<S, T, KF_FORCE, R><<<grid, RING_W, L::bytes, s>>>(doms, maps, units, nunits, parity,
-                                                                        counters);
+        k_batch_ring<S, T, KF_FORCE, R, W><<<grid, W, L::bytes, s>>>(doms, maps, units, nunits, parity,
+                                                                      counters);
     else
-        k_batch_ring<S, T, 0, R><<<grid, RING_W, L::bytes, s>>>(doms, maps, units, nunits, parity, counters);
+        k_batch_ring<S, T, 0, R, W><<<grid, W, L::bytes, s>>>(doms, maps, units, nunits, parity, counters);
     return cudaGetLastError();
 }
 

@@ -145,19 +145,21 @@ struct RingMaps;
 struct RingUnit;
 cudaError_t launch_batch_ring_fp64(const Fused2Args<double, double> *doms, const RingMaps *maps,
                                    const RingUnit *units, int nunits, int parity, int grid, int flags,
-                                   unsigned *counters, cudaStream_t s);
+                                   unsigned *counters, int width, cudaStream_t s);
 cudaError_t launch_batch_ring_f32(const Fused2Args<float, float> *doms, const RingMaps *maps,
                                   const RingUnit *units, int nunits, int parity, int grid, int flags,
-                                  unsigned *counters, cudaStream_t s);
+                                  unsigned *counters, int width, cudaStream_t s);
 cudaError_t launch_batch_ring_f16(const Fused2Args<__half, float> *doms, const RingMaps *maps,
                                   const RingUnit *units, int nunits, int parity, int grid, int flags,
-                                  unsigned *counters, cudaStream_t s);
+                                  unsigned *counters, int width, cudaStream_t s);
 // shared-memory limits and resident CTAs per SM of the batched ring kernel
-int batch_ring_prepare(sclbm_precision p, int *per_sm);
-// tensor maps of a domain's argument block (host); 0 on success
-int ring_maps_of(const Fused2Args<double, double> &a, RingMaps *m);
-int ring_maps_of(const Fused2Args<float, float> &a, RingMaps *m);
-int ring_maps_of(const Fused2Args<__half, float> &a, RingMaps *m);
+// with strips `width` (128 or 64) columns wide
+int batch_ring_prepare(sclbm_precision p, int width, int *per_sm);
+// tensor maps of a domain's argument block for strips `width` columns wide
+// (host); 0 on success
+int ring_maps_of(const Fused2Args<double, double> &a, int width, RingMaps *m);
+int ring_maps_of(const Fused2Args<float, float> &a, int width, RingMaps *m);
+int ring_maps_of(const Fused2Args<__half, float> &a, int width, RingMaps *m);
 int async_resident_fp64(); // CTAs of the batched kernel resident on the device
 int async_resident_f32();
 constexpr int ASYNC_STRIP = 128;

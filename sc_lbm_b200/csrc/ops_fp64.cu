@@ -447,20 +447,26 @@ cudaError_t launch_ring2_fp64(const Fused2Args<double, double> &a, int stages, c
 constexpr int RING_BATCH_R64 = 3;
 cudaError_t launch_batch_ring_fp64(const Fused2Args<double, double> *doms, const RingMaps *maps,
                                    const RingUnit *units, int nunits, int parity, int grid, int flags,
-                                   unsigned *counters, cudaStream_t s)
+                                   unsigned *counters, int width, cudaStream_t s)
 {
-    return launch_batch_ring<double, double, RING_BATCH_R64, 0>(doms, maps, units, nunits, parity, grid,
-                                                                 flags, counters, s);
+    if (width == 64)
+        return launch_batch_ring<double, double, RING_BATCH_R64, 0, 64>(doms, maps, units, nunits, parity,
+                                                                         grid, flags, counters, s);
+    return launch_batch_ring<double, double, RING_BATCH_R64, 0, 128>(doms, maps, units, nunits, parity,
+                                                                      grid, flags, counters, s);
 }
-int batch_ring_prepare_shifted(sclbm_precision p, int *per_sm);
-int batch_ring_prepare(sclbm_precision p, int *per_sm)
+int batch_ring_prepare_shifted(sclbm_precision p, int width, int *per_sm);
+int batch_ring_prepare(sclbm_precision p, int width, int *per_sm)
 {
-    if (p != SCLBM_FP64) return batch_ring_prepare_shifted(p, per_sm);
-    const cudaError_t e = batch_ring_prepare<double, double, RING_BATCH_R64, 0>(per_sm);
+    if (p != SCLBM_FP64) return batch_ring_prepare_shifted(p, width, per_sm);
+    const cudaError_t e = width == 64 ? batch_ring_prepare<double, double, RING_BATCH_R64, 0, 64>(per_sm)
+                                      : batch_ring_prepare<double, double, RING_BATCH_R64, 0, 128>(per_sm);
     return e == cudaSuccess ? 0 : cuda_fail(e, "ring batch set-up");
 }
-int ring_maps_of(const Fused2Args<double, double> &a, RingMaps *m)
+int ring_maps_of(const Fused2Args<double, double> &a, int width, RingMaps *m)
 {
-    return ring_maps<double, double, RING_BATCH_R64>(a, *m) == cudaSuccess ? 0 : 1;
+    const cudaError_t e = width == 64 ? ring_maps<double, double, RING_BATCH_R64, 64>(a, *m)
+                                      : ring_maps<double, double, RING_BATCH_R64, 128>(a, *m);
+    return e == cudaSuccess ? 0 : 1;
 }
 } // namespace sclbm

@@ -114,36 +114,51 @@ cudaError_t launch_ring2_f16(const Fused2Args<__half, float> &a, int stages, cud
     if (stages > 0) return launch_ring2_any<__half, float, 6>(a, s);
     return launch_ring2_any<__half, float, 5>(a, s);
 }
-// batches: the single-domain depths, uniform solid form
+// batches: the single-domain depths, uniform solid form; strips 128 or 64
+// columns wide
 constexpr int RING_BATCH_R32 = 3, RING_BATCH_R16 = 5;
 cudaError_t launch_batch_ring_f32(const Fused2Args<float, float> *doms, const RingMaps *maps,
                                   const RingUnit *units, int nunits, int parity, int grid, int flags,
-                                  unsigned *counters, cudaStream_t s)
+                                  unsigned *counters, int width, cudaStream_t s)
 {
-    return launch_batch_ring<float, float, RING_BATCH_R32, KF_UNIFORM>(doms, maps, units, nunits, parity,
-                                                                       grid, flags, counters, s);
+    if (width == 64)
+        return launch_batch_ring<float, float, RING_BATCH_R32, KF_UNIFORM, 64>(doms, maps, units, nunits,
+                                                                               parity, grid, flags, counters, s);
+    return launch_batch_ring<float, float, RING_BATCH_R32, KF_UNIFORM, 128>(doms, maps, units, nunits,
+                                                                            parity, grid, flags, counters, s);
 }
 cudaError_t launch_batch_ring_f16(const Fused2Args<__half, float> *doms, const RingMaps *maps,
                                   const RingUnit *units, int nunits, int parity, int grid, int flags,
-                                  unsigned *counters, cudaStream_t s)
+                                  unsigned *counters, int width, cudaStream_t s)
 {
-    return launch_batch_ring<__half, float, RING_BATCH_R16, KF_UNIFORM>(doms, maps, units, nunits, parity,
-                                                                        grid, flags, counters, s);
+    if (width == 64)
+        return launch_batch_ring<__half, float, RING_BATCH_R16, KF_UNIFORM, 64>(doms, maps, units, nunits,
+                                                                                parity, grid, flags, counters, s);
+    return launch_batch_ring<__half, float, RING_BATCH_R16, KF_UNIFORM, 128>(doms, maps, units, nunits,
+                                                                             parity, grid, flags, counters, s);
 }
-int batch_ring_prepare_shifted(sclbm_precision p, int *per_sm)
+int batch_ring_prepare_shifted(sclbm_precision p, int width, int *per_sm)
 {
-    const cudaError_t e = p == SCLBM_FP32_SHIFTED
-                              ? batch_ring_prepare<float, float, RING_BATCH_R32, KF_UNIFORM>(per_sm)
-                              : batch_ring_prepare<__half, float, RING_BATCH_R16, KF_UNIFORM>(per_sm);
+    cudaError_t e;
+    if (p == SCLBM_FP32_SHIFTED)
+        e = width == 64 ? batch_ring_prepare<float, float, RING_BATCH_R32, KF_UNIFORM, 64>(per_sm)
+                        : batch_ring_prepare<float, float, RING_BATCH_R32, KF_UNIFORM, 128>(per_sm);
+    else
+        e = width == 64 ? batch_ring_prepare<__half, float, RING_BATCH_R16, KF_UNIFORM, 64>(per_sm)
+                        : batch_ring_prepare<__half, float, RING_BATCH_R16, KF_UNIFORM, 128>(per_sm);
     return e == cudaSuccess ? 0 : cuda_fail(e, "ring batch set-up");
 }
-int ring_maps_of(const Fused2Args<float, float> &a, RingMaps *m)
+int ring_maps_of(const Fused2Args<float, float> &a, int width, RingMaps *m)
 {
-    return ring_maps<float, float, RING_BATCH_R32>(a, *m) == cudaSuccess ? 0 : 1;
+    const cudaError_t e = width == 64 ? ring_maps<float, float, RING_BATCH_R32, 64>(a, *m)
+                                      : ring_maps<float, float, RING_BATCH_R32, 128>(a, *m);
+    return e == cudaSuccess ? 0 : 1;
 }
-int ring_maps_of(const Fused2Args<__half, float> &a, RingMaps *m)
+int ring_maps_of(const Fused2Args<__half, float> &a, int width, RingMaps *m)
 {
-    return ring_maps<__half, float, RING_BATCH_R16>(a, *m) == cudaSuccess ? 0 : 1;
+    const cudaError_t e = width == 64 ? ring_maps<__half, float, RING_BATCH_R16, 64>(a, *m)
+                                      : ring_maps<__half, float, RING_BATCH_R16, 128>(a, *m);
+    return e == cudaSuccess ? 0 : 1;
 }
 } // namespace sclbm
 

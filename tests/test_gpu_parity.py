@@ -286,7 +286,8 @@ def test_batch_matches_individual_domains(sclbm):
                                 (sclbm.FP16_SHIFTED, False, 9), (sclbm.FP32_SHIFTED, True, 10),
                                 (sclbm.FP16_SHIFTED, False, 10), (sclbm.FP32_SHIFTED, True, 11),
                                 (sclbm.FP16_SHIFTED, True, 11), (sclbm.FP64, True, 11),
-                                (sclbm.FP32_SHIFTED, False, 11)):
+                                (sclbm.FP32_SHIFTED, False, 11), (sclbm.FP32_SHIFTED, True, 12),
+                                (sclbm.FP16_SHIFTED, True, 12), (sclbm.FP64, False, 12)):
         rr = (0.8, 1.2)
         solo = [gpu_runner.run_domain(sclbm, dict(RUNS[n], steps=45), prec, rho_ref=rr) for n in names]
         doms = [gpu_runner.make_domain(sclbm, RUNS[n], prec, rho_ref=rr) for n in names]
@@ -298,7 +299,7 @@ def test_batch_matches_individual_domains(sclbm):
                 assert d.download_f(k).tobytes() == s[f"c{k + 1}_f"].tobytes(), (prec, n, k)
 
 
-@pytest.mark.parametrize("kernel", [0, 11])
+@pytest.mark.parametrize("kernel", [0, 11, 12])
 def test_batch_fp64_matches_reference(sclbm, kernel):
     names = ["porous_96x48", "spinodal_48x40", "laplace_64x64"]
     doms = [gpu_runner.make_domain(sclbm, RUNS[n], sclbm.FP64) for n in names]

@@ -51,7 +51,8 @@ struct sclbm_batch {
     // of (domain, strip, band), tensor maps per domain and parity, the work
     // counters; absent when a domain's rows do not start on 16-byte boundaries
     bool ring = false;
-    int use_ring = 0; // 0, or the strip width of the ring body in use
+    int use_ring = 0;  // 0, or the strip width of the ring body in use
+    int auto_ring = 0; // the ring body of variant 0
     RingUnit *d_units[2] = {nullptr, nullptr}; // [0] 128 wide, [1] 64 wide
     RingMaps *d_maps[2] = {nullptr, nullptr};
     unsigned *d_counters = nullptr;
@@ -302,6 +303,11 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
                                                                    : BODY_UNIFORM;
     b->body = b->auto_body;
     b->use_units = b->auto_units;
+    // FP32/FP64 batches with solid nodes: the ring body on 128-column strips
+    // (512-domain ensemble: FP32 24.5 vs 21.3 GLUPS for the uniform tile list,
+    // FP64 12.0 vs 10.3; FP16 keeps its one-warp tile list, 24.9 vs 24.1)
+    b->auto_ring = b->ring && (b->flags & KF_SOLID) && b->prec != SCLBM_FP16_SHIFTED ? 128 : 0;
+    b->use_ring = b->auto_ring;
     std::vector<BandTile> bands;
     if (b->prec != SCLBM_FP16_SHIFTED) {
         const int res = std::max(1, b->prec == SCLBM_FP64 ? async_resident_fp64() : async_resident_f32());
@@ -370,7 +376,7 @@ int sclbm_batch_set_kernel(sclbm_batch *b, int variant)
     if ((variant == 5 || variant == 6 || (variant >= 8 && variant <= 10)) && b->prec == SCLBM_FP64)
         return set_error(SCLBM_E_INVALID_ARGUMENT,
                          "the load-ahead, compacted and uniform tile lists are for FP32/FP16 storage");
-    b->use_ring = variant == 11 ? 128 : (variant == 12 ? 64 : 0);
+    b->use_ring = variant == 11 ? 128 : (variant == 12 ? 64 : (variant == 0 ? b->auto_ring : 0));
     b->use_units = variant == 3 || (variant == 0 && b->auto_units);
     b->body = variant == 5   ? BODY_AHEAD
               : variant == 6 ? BODY_COMPACT

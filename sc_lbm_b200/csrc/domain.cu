@@ -337,9 +337,17 @@ static cudaError_t step_one(const sclbm_domain *d, cudaStream_t s)
     // (FP64 at 4096^2: register tile 17.4 GLUPS all-fluid, 15.4 at 60 % fluid,
     // against 16.4 and 14.8 for the pipelined kernel); 3 and 9 force the
     // pipelined kernel
-    // 11, 12, 13: the ring kernel (bulk row copies into shared memory) with its
-    // default, fewer and more stages; lattices whose rows do not start on
-    // 16-byte boundaries take the register tile
+    // 11, 12, 13: the ring kernel (rows streamed into shared memory by tensor
+    // copies) with its default, fewer and more stages; lattices whose rows do
+    // not start on 16-byte boundaries take the register tile.  Variant 0 runs
+    // it on FP32 and FP64 lattices with solid nodes (4096^2, 60 % fluid, with
+    // force: FP32 0.498 ms with four stages against 0.542 for the uniform
+    // register tile; FP64 0.955 with three against 1.061); all-fluid lattices
+    // and FP16 storage keep the register tile, which is faster there
+    if (d->variant == 0 && d->has_solid && sizeof(S) != 2 && ring_row_aligned(d)) {
+        if constexpr (sizeof(S) == 8) return launch_ring2_fp64(a, 0, s);
+        else if constexpr (sizeof(S) == 4) return launch_ring2_f32(a, 1, s);
+    }
     if (d->variant >= 11 && d->variant <= 13 && ring_row_aligned(d)) {
         const int st = d->variant == 11 ? 0 : (d->variant == 12 ? -1 : 1);
         if constexpr (sizeof(S) == 8) return launch_ring2_fp64(a, st, s);

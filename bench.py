@@ -409,6 +409,9 @@ def run_ensemble(torch, sc, stream, steps, warmup, single_mlups, ranks, n=512):
     nodes = sum(d.N for d in doms)
     b = sc.Batch(doms)
     ntiles, grid = b.info()
+    # the first 20 steps capture and instantiate the batch's CUDA graph: keep
+    # that out of the timed region
+    b.step(20)
     b.step(warmup)
     ranks.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -33,6 +33,8 @@ def main():
     ap.add_argument("--porosity", type=float, default=1.0,
                     help="< 1: seeded disks of radius 8-20 and walls top and bottom")
     ap.add_argument("--force", action="store_true", help="body force 1e-5 along x on component 1")
+    ap.add_argument("--disks", type=int, nargs=2, default=[8, 20], metavar=("RMIN", "RMAX"),
+                    help="disk radii of --porosity (2 8: the ensemble's geometry, no walls)")
     ap.add_argument("--ensemble", type=int, default=0,
                     help="> 0: time a batch of that many seeded ensemble domains instead")
     args = ap.parse_args()
@@ -59,7 +61,11 @@ def main():
     else:
         N = args.nx * args.ny
         if args.porosity < 1.0:
-            mask, _, _ = W.disk_mask(args.nx, args.ny, args.porosity, 8, 20, 11, walls="x")
+            if args.disks == [8, 20]:
+                mask, _, _ = W.disk_mask(args.nx, args.ny, args.porosity, 8, 20, 11, walls="x")
+            else:
+                mask, _, _ = W.disk_mask(args.nx, args.ny, args.porosity, args.disks[0], args.disks[1],
+                                         31337, max_tries=400000, max_misses=2000)
         else:
             mask = np.ones(N, np.int32)
         rng = np.random.default_rng(1)

@@ -345,14 +345,14 @@ static cudaError_t step_one(const sclbm_domain *d, cudaStream_t s)
     // register tile; FP64 0.955 with three against 1.061); all-fluid lattices
     // and FP16 storage keep the register tile, which is faster there
     if (d->variant == 0 && d->has_solid && sizeof(S) != 2 && ring_row_aligned(d)) {
-        if constexpr (sizeof(S) == 8) return launch_ring2_fp64(a, 0, s);
-        else if constexpr (sizeof(S) == 4) return launch_ring2_f32(a, 1, s);
+        if constexpr (sizeof(S) == 8) return launch_ring2_fp64(a, 0, d->tile_y, s);
+        else if constexpr (sizeof(S) == 4) return launch_ring2_f32(a, 1, d->tile_y, s);
     }
     if (d->variant >= 11 && d->variant <= 13 && ring_row_aligned(d)) {
         const int st = d->variant == 11 ? 0 : (d->variant == 12 ? -1 : 1);
-        if constexpr (sizeof(S) == 8) return launch_ring2_fp64(a, st, s);
-        else if constexpr (sizeof(S) == 4) return launch_ring2_f32(a, st, s);
-        else return launch_ring2_f16(a, st, s);
+        if constexpr (sizeof(S) == 8) return launch_ring2_fp64(a, st, d->tile_y, s);
+        else if constexpr (sizeof(S) == 4) return launch_ring2_f32(a, st, d->tile_y, s);
+        else return launch_ring2_f16(a, st, d->tile_y, s);
     }
     const bool pipelined = d->variant == 3 || d->variant == 9;
     if (pipelined) {

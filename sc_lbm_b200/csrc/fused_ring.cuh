@@ -443,8 +443,12 @@ inline cudaError_t ring_maps(const Fused2Args<S, T> &a, RingMaps &m)
     return cudaSuccess;
 }
 
+// rows: rows per band (0: bands sized for about RING_WAVES waves of the
+// resident CTAs -- several waves let the block scheduler even out bands whose
+// fluid nodes, and so whose work, differ)
+constexpr int RING_WAVES = 4;
 template <typename S, typename T, int FLAGS, int R, bool WIDE>
-inline cudaError_t launch_ring2_f(const Fused2Args<S, T> &a, cudaStream_t s)
+inline cudaError_t launch_ring2_f(const Fused2Args<S, T> &a, int rows, cudaStream_t s)
 {
     using L = RingLayout<S, T, R>;
     auto kern = k_ring2<S, T, FLAGS, R, WIDE>;
@@ -460,9 +464,9 @@ inline cudaError_t launch_ring2_f(const Fused2Args<S, T> &a, cudaStream_t s)
     }
     const int strips = (a.nx + RING_W - 1) / RING_W;
     const int resident = per_sm * sm_count();
-    // one wave: as many bands as resident CTAs allow, at least 4 rows each
-    int bands = std::max(1, resident / strips);
-    bands = std::min(bands, std::max(1, a.ny / 4));
+    int bands = rows > 0 ? (a.ny + rows - 1) / rows : std::max(1, RING_WAVES * resident / strips);
+    bands = std::min(bands, std::max(1, a.ny / 4)); // at least 4 rows a band
+    bands = std::min(bands, 65535);                 // grid y limit
     RingMaps maps;
     const cudaError_t em = ring_maps<S, T, R>(a, maps);
     if (em != cudaSuccess) return em;
@@ -476,15 +480,15 @@ template <typename S> inline bool ring_fits(int nx) { return nx % ring_pad<S>() 
 
 // UNI: lattices with solid nodes run the uniform solid form (KF_UNIFORM)
 template <typename S, typename T, int R, int UNI = KF_UNIFORM>
-inline cudaError_t launch_ring2_any(const Fused2Args<S, T> &a, cudaStream_t s)
+inline cudaError_t launch_ring2_any(const Fused2Args<S, T> &a, int rows, cudaStream_t s)
 {
     if (!ring_fits<S>(a.nx) || a.nx < 1 || a.ny < 1) return cudaErrorInvalidValue;
-    if (needs_wide_offsets(a.N)) return launch_ring2_f<S, T, KF_FORCE | KF_SOLID | UNI, R, true>(a, s);
+    if (needs_wide_offsets(a.N)) return launch_ring2_f<S, T, KF_FORCE | KF_SOLID | UNI, R, true>(a, rows, s);
     switch (kernel_flags(a)) {
-    case 0: return launch_ring2_f<S, T, 0, R, false>(a, s);
-    case KF_FORCE: return launch_ring2_f<S, T, KF_FORCE, R, false>(a, s);
-    case KF_SOLID: return launch_ring2_f<S, T, KF_SOLID | UNI, R, false>(a, s);
-    default: return launch_ring2_f<S, T, KF_FORCE | KF_SOLID | UNI, R, false>(a, s);
+    case 0: return launch_ring2_f<S, T, 0, R, false>(a, rows, s);
+    case KF_FORCE: return launch_ring2_f<S, T, KF_FORCE, R, false>(a, rows, s);
+    case KF_SOLID: return launch_ring2_f<S, T, KF_SOLID | UNI, R, false>(a, rows, s);
+    default: return launch_ring2_f<S, T, KF_FORCE | KF_SOLID | UNI, R, false>(a, rows, s);
     }
 }
 

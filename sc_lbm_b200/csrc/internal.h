@@ -132,12 +132,12 @@ cudaError_t launch_batch2_async_fp64(const Fused2Args<double, double> *doms, con
 cudaError_t launch_batch2_async_f32(const Fused2Args<float, float> *doms, const BandTile *tiles,
                                     int ntiles, int grid, int parity, cudaStream_t s);
 // ring kernels (fused_ring.cuh): population rows streamed into shared memory
-// by bulk asynchronous copies; stages selects the ring depth (0 default, -1
-// fewer, +1 more); cudaErrorInvalidValue when nx is not a multiple of
-// 16 / sizeof(storage)
-cudaError_t launch_ring2_fp64(const Fused2Args<double, double> &a, int stages, cudaStream_t s);
-cudaError_t launch_ring2_f32(const Fused2Args<float, float> &a, int stages, cudaStream_t s);
-cudaError_t launch_ring2_f16(const Fused2Args<__half, float> &a, int stages, cudaStream_t s);
+// by tensor copies; stages selects the ring depth (0 default, -1 fewer, +1
+// more), rows the rows per band (0 default); cudaErrorInvalidValue when nx is
+// not a multiple of 16 / sizeof(storage)
+cudaError_t launch_ring2_fp64(const Fused2Args<double, double> &a, int stages, int rows, cudaStream_t s);
+cudaError_t launch_ring2_f32(const Fused2Args<float, float> &a, int stages, int rows, cudaStream_t s);
+cudaError_t launch_ring2_f16(const Fused2Args<__half, float> &a, int stages, int rows, cudaStream_t s);
 // batched ring kernel (fused_ring.cuh): maps and units are device arrays
 // (RingMaps per domain and parity; RingUnit work list); counters: two
 // device words, zero before the first launch

@@ -102,17 +102,17 @@ int batch_blocks_per_sm(sclbm_precision p, int body)
 namespace sclbm {
 // FP32: 9.8 KB per stage; three stages (34 KB) keep the six CTAs per SM that
 // the registers allow.  FP16: 5.2 KB per stage, five stages.
-cudaError_t launch_ring2_f32(const Fused2Args<float, float> &a, int stages, cudaStream_t s)
+cudaError_t launch_ring2_f32(const Fused2Args<float, float> &a, int stages, int rows, cudaStream_t s)
 {
-    if (stages < 0) return launch_ring2_any<float, float, 2>(a, s);
-    if (stages > 0) return launch_ring2_any<float, float, 4>(a, s);
-    return launch_ring2_any<float, float, 3>(a, s);
+    if (stages < 0) return launch_ring2_any<float, float, 2>(a, rows, s);
+    if (stages > 0) return launch_ring2_any<float, float, 4>(a, rows, s);
+    return launch_ring2_any<float, float, 3>(a, rows, s);
 }
-cudaError_t launch_ring2_f16(const Fused2Args<__half, float> &a, int stages, cudaStream_t s)
+cudaError_t launch_ring2_f16(const Fused2Args<__half, float> &a, int stages, int rows, cudaStream_t s)
 {
-    if (stages < 0) return launch_ring2_any<__half, float, 4>(a, s);
-    if (stages > 0) return launch_ring2_any<__half, float, 6>(a, s);
-    return launch_ring2_any<__half, float, 5>(a, s);
+    if (stages < 0) return launch_ring2_any<__half, float, 4>(a, rows, s);
+    if (stages > 0) return launch_ring2_any<__half, float, 6>(a, rows, s);
+    return launch_ring2_any<__half, float, 5>(a, rows, s);
 }
 // batches: the single-domain depths, uniform solid form; strips 128 or 64
 // columns wide

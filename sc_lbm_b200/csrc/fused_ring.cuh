@@ -14,11 +14,11 @@
 // engine's per-copy cost dominated at 300-1000 bytes a copy).
 //
 // Work decomposition.  A CTA of RING_W threads owns a strip of RING_W interior
-// columns and a band of rows; the bands split every strip at the same rows
-// and are sized so that every CTA of the grid is resident at once (one wave,
-// no tail).  Neighbouring bands march in opposite directions, so the two
-// halo rows that a pair of bands shares are read by both near the same time
-// and the second read hits L2.
+// columns and a band of rows (32 by default: several waves of CTAs, which the
+// block scheduler balances where bands hold different numbers of fluid
+// nodes).  Neighbouring bands march in opposite directions, so the two halo
+// rows that a pair of bands shares are read by both near the same time and
+// the second read often hits L2.
 //
 // Ring.  Row j of a band (j = 0 .. nrow+1, halo rows included) lands in stage
 // j % R: per component a box of 9 directions x P = RING_W + 2A elements,
@@ -443,16 +443,19 @@ inline cudaError_t ring_maps(const Fused2Args<S, T> &a, RingMaps &m)
     return cudaSuccess;
 }
 
-// rows: rows per band (0: bands sized for about RING_WAVES waves of the
-// resident CTAs -- several waves let the block scheduler even out bands whose
-// fluid nodes, and so whose work, differ)
-constexpr int RING_WAVES = 4;
+// rows: rows per band (0: RING_ROWS).  Bands of 32 rows give 4096^2 lattices
+// about four waves of CTAs, which lets the block scheduler even out bands
+// whose fluid nodes, and so whose work, differ: on porous 4096^2 lattices one
+// wave of tall bands ran 5-25 % slower than 32-row bands, 128-row bands
+// 3-14 % slower (FP32 and FP64, disks of radius 8-20 at 60 % fluid and 2-8
+// at 72 %).
+constexpr int RING_ROWS = 32;
 template <typename S, typename T, int FLAGS, int R, bool WIDE>
 inline cudaError_t launch_ring2_f(const Fused2Args<S, T> &a, int rows, cudaStream_t s)
 {
     using L = RingLayout<S, T, R>;
     auto kern = k_ring2<S, T, FLAGS, R, WIDE>;
-    static int per_sm = 0; // resident CTAs per SM of this instantiation (one device)
+    static int per_sm = 0; // resident CTAs per SM of this instantiation (one device): >= 1 checked once
     if (per_sm == 0) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes);
         if (e != cudaSuccess) return e;
@@ -463,8 +466,8 @@ inline cudaError_t launch_ring2_f(const Fused2Args<S, T> &a, int rows, cudaStrea
         per_sm = n;
     }
     const int strips = (a.nx + RING_W - 1) / RING_W;
-    const int resident = per_sm * sm_count();
-    int bands = rows > 0 ? (a.ny + rows - 1) / rows : std::max(1, RING_WAVES * resident / strips);
+    const int r = rows > 0 ? rows : RING_ROWS;
+    int bands = (a.ny + r - 1) / r;
     bands = std::min(bands, std::max(1, a.ny / 4)); // at least 4 rows a band
     bands = std::min(bands, 65535);                 // grid y limit
     RingMaps maps;

@@ -11,7 +11,7 @@ path:
     sum over fluid neighbours of w c psi = sum w c drho_nbr - rho_ref * S,
         S = sum over solid neighbours of w c (the solid-force sums)
     d_eq_i = w_i (drho + rho (3 c.u + 4.5 (c.u)^2 - 1.5 u^2))
-    d*_i   = d_i + omega (d_eq_i - d_i) [+ F_i]     (i = 1..8)
+    d*_i   = d_i + omega (d_eq_i - d_i) [+ F_i]     (i = 1..8, rounded to storage)
     d*_0   = d_0 + sum_{i>=1} (d_i - d*_i) [+ sum_i F_i]   (the rest population
              closes the node's mass, as the kernel does: equal to the BGK
              value in exact arithmetic)
@@ -72,7 +72,7 @@ def step(d, mask, p, store=np.float32, compute=np.float32):
             v = x[k][i] + om[k] * (fe - x[k][i])
             if p["force"][k] is not None:
                 v = v + T(p["force"][k][i])
-            v = np.where(mask, v, T(0))
+            v = np.where(mask, v, T(0)).astype(store).astype(T)
             out[k][i] = v
             rest = rest + (x[k][i] - v)
         out[k][0] = np.where(mask, rest, T(0))

@@ -14,8 +14,18 @@ over the candidate shapes of each storage precision:
 It then runs one member of the class in FP64 and in the shifted forms for
 `--accuracy-steps` steps and records max|drho|/mean(rho) against FP64; the
 recommended storage of the class is the fastest whose error stays within
-`--tolerance` (1e-5).  The JSON it writes is compiled into the library by
-build.py (sclbm_tuned_config, and the batch defaults).
+`--tolerance` (1e-5).
+
+Finally it times what a batch actually runs on the benchmark's mixed workload:
+the whole seeded 512-domain ensemble (sizes, porosities and parameters mixed
+as the configuration draws them) in one batch, for every batch body -- the
+ring bodies (variants 11 and 12: 128- and 64-column strips) at several rows
+per unit, the tile lists (2 register tile, 8 uniform solid form, 9 half
+tiles, 10 one-warp tiles) at several rows per tile, and the strips x bands
+body (3) -- per storage precision.  The fastest becomes the `batch_default`
+of that precision, the body every batch with solid nodes starts with.  The
+JSON it writes is compiled into the library by build.py (sclbm_tuned_config,
+the size-class tile heights and the batch defaults).
 """
 from __future__ import annotations
 
@@ -56,7 +66,7 @@ def make_domains(sc, W, nx, ny, prec, count, distinct=8, seed=4242):
 def time_batch(torch, sc, stream, doms, variant, tile_y, steps, warmup):
     b = sc.Batch(doms, tile_y=[tile_y] * len(doms))
     b.set_kernel(variant)
-    b.step(warmup)
+    b.step(max(warmup, 20))  # builds the 20-step CUDA graph outside the timed steps
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -87,6 +97,39 @@ def accuracy(sc, W, member, steps):
                         for k in range(2))
     out["fp64"] = 0.0
     return out
+
+
+# candidates of the mixed-ensemble sweep: (variant, rows per unit / tile)
+ENSEMBLE_CANDIDATES = {
+    "fp64": [(11, 16), (11, 24), (11, 32), (11, 48), (11, 64), (12, 32), (2, 16), (2, 32), (3, 0)],
+    "fp32s": [(11, 16), (11, 24), (11, 32), (11, 48), (11, 64), (12, 32), (2, 16), (8, 16), (8, 32),
+              (9, 16), (10, 16), (10, 32), (3, 0)],
+    "fp16s": [(11, 16), (11, 32), (11, 64), (12, 32), (2, 32), (8, 16), (8, 32), (10, 16), (10, 32)],
+}
+
+
+def ensemble_sweep(torch, sc, W, stream, steps, warmup, n=512):
+    """Mixed-ensemble timings per precision and the fastest body of each."""
+    members = W.ensemble(n)
+    sweep, best = {}, {}
+    for prec, pname in ((sc.FP64, "fp64"), (sc.FP32_SHIFTED, "fp32s"), (sc.FP16_SHIFTED, "fp16s")):
+        doms = []
+        for m in members:
+            d = sc.Domain(m["nx"], m["ny"], m["mask"], W.params_of(m, sc), prec)
+            d.upload_f(0, m["f1"])
+            d.upload_f(1, m["f2"])
+            doms.append(d)
+        res = []
+        for variant, rows in ENSEMBLE_CANDIDATES[pname]:
+            mlups, ms = time_batch(torch, sc, stream, doms, variant, rows or 16, steps, warmup)
+            res.append({"variant": variant, "rows": rows, "mlups": round(mlups, 1),
+                        "ms_per_step": round(ms, 5)})
+            print(json.dumps({"ensemble": pname, **res[-1]}), flush=True)
+        sweep[pname] = res
+        top = max(res, key=lambda r: r["mlups"])
+        best[pname] = {"variant": top["variant"], "rows": top["rows"], "mlups": top["mlups"]}
+        del doms
+    return sweep, best
 
 
 def select(results, margin):
@@ -125,6 +168,8 @@ def main():
                     help="shapes within this fraction of the fastest count as equal")
     ap.add_argument("--reselect", action="store_true",
                     help="re-apply the selection rule to the sweep in --out and exit")
+    ap.add_argument("--ensemble-only", action="store_true",
+                    help="only the mixed-ensemble sweep, merged into the existing --out")
     args = ap.parse_args()
     if args.reselect:
         reselect(args.out, args.margin)
@@ -139,6 +184,16 @@ def main():
     sc.set_stream(stream.cuda_stream)
     props = torch.cuda.get_device_properties(0)
     t_start = time.time()
+    if args.ensemble_only:
+        with open(args.out) as fh:
+            out = json.load(fh)
+        out["ensemble_sweep"], out["batch_default"] = ensemble_sweep(torch, sc, W, stream, args.steps,
+                                                                     args.warmup)
+        out["ensemble_command"] = "python -m sc_lbm_b200.autotune " + " ".join(sys.argv[1:])
+        with open(args.out, "w") as fh:
+            json.dump(out, fh, indent=1)
+        print(f"wrote {args.out}")
+        return
     classes = []
     for i in range(len(NX_EDGES) - 1):
         for j in range(len(NY_EDGES) - 1):
@@ -179,6 +234,9 @@ def main():
                    "variant 2 = tile list, 3 = strips x bands; mlups of a batch of "
                    "`domains` seeded porous domains of the representative size",
            "classes": classes}
+    out["ensemble_sweep"], out["batch_default"] = ensemble_sweep(torch, sc, W, stream, args.steps,
+                                                                 args.warmup)
+    out["seconds"] = round(time.time() - t_start, 1)
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     with open(args.out, "w") as fh:
         json.dump(out, fh, indent=1)

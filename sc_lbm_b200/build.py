@@ -34,10 +34,12 @@ def tuned_table_source(path: str = TUNING_JSON) -> str:
     import json
     lines = [f"// generated by sc_lbm_b200/build.py from {os.path.relpath(path, ROOT)}",
              "#pragma once", "// included after tuning.h (SclbmTunedClass)"]
-    classes = []
+    classes, batch = [], {}
     if os.path.exists(path):
         with open(path) as fh:
-            classes = json.load(fh).get("classes", [])
+            d = json.load(fh)
+        classes = d.get("classes", [])
+        batch = d.get("batch_default", {})
     rows = []
     for c in classes:
         shapes = ", ".join("{%d, %d}" % (int(c["shapes"][p]["variant"]), int(c["shapes"][p]["tile_y"]))
@@ -48,6 +50,11 @@ def tuned_table_source(path: str = TUNING_JSON) -> str:
     lines.append("static const SclbmTunedClass kSclbmTuned[%d] = {" % max(1, len(rows)))
     lines += rows or ["    {0, 0, 0, 0, 0, {{0, 0}, {0, 0}, {0, 0}}},"]
     lines.append("};")
+    # the body the mixed-ensemble sweep found fastest for batches with solid
+    # nodes, per storage precision ({0, 0}: the size-class table decides)
+    bd = ", ".join("{%d, %d}" % (int(batch.get(p, {}).get("variant", 0)), int(batch.get(p, {}).get("rows", 0)))
+                   for p in PRECISIONS)
+    lines.append("static const SclbmTunedShape kSclbmBatchDefault[3] = {%s};" % bd)
     return "\n".join(lines) + "\n"
 
 

@@ -111,14 +111,15 @@ static cudaError_t batch_launch_any(sclbm_batch *b, int parity, cudaStream_t s)
 // about `rows` rows (a domain's bands alternate their march direction),
 // largest units first; tensor maps of both parities of every domain.
 template <typename S, typename T>
-static int build_ring(sclbm_batch *b, const std::vector<Fused2Args<S, T>> &h, int rows, int width)
+static int build_ring(sclbm_batch *b, const std::vector<Fused2Args<S, T>> &h, const std::vector<int> &rows,
+                      int width)
 {
     const int r = width == 64 ? 1 : 0;
     std::vector<RingUnit> units;
     std::vector<long> cost;
     for (int k = 0; k < (int)b->doms.size(); ++k) {
         const sclbm_domain *d = b->doms[k];
-        const int nb = std::max(1, (int)((d->ny + rows / 2) / rows));
+        const int nb = std::max(1, (int)((d->ny + rows[k] / 2) / rows[k]));
         for (int j = 0; j < nb; ++j) {
             const int y0 = (int)((long long)d->ny * j / nb), y1 = (int)((long long)d->ny * (j + 1) / nb);
             for (int xb = 0; xb < (int)d->nx; xb += width) {
@@ -149,7 +150,7 @@ static int build_ring(sclbm_batch *b, const std::vector<Fused2Args<S, T>> &h, in
 }
 
 template <typename S, typename T>
-static int build_rings(sclbm_batch *b, const std::vector<Fused2Args<S, T>> &h, int rows)
+static int build_rings(sclbm_batch *b, const std::vector<Fused2Args<S, T>> &h, const std::vector<int> &rows)
 {
     const int A = 16 / (int)sizeof(S);
     for (auto *d : b->doms)
@@ -163,11 +164,12 @@ static int build_rings(sclbm_batch *b, const std::vector<Fused2Args<S, T>> &h, i
     return SCLBM_OK;
 }
 
-// rows per unit of the ring body (a unit reads two halo rows)
+// rows per unit of the ring body (a unit reads two halo rows), unless the
+// caller gives tile_y per domain or the tuned batch default sets them
 constexpr int RING_BATCH_ROWS = 32;
 
 template <typename S, typename T>
-static int upload_args(sclbm_batch *b, const std::vector<int> &ty)
+static int upload_args(sclbm_batch *b, const std::vector<int> &ty, const std::vector<int> &ring_rows)
 {
     std::vector<Fused2Args<S, T>> h(2 * b->doms.size());
     for (size_t k = 0; k < b->doms.size(); ++k) {
@@ -190,7 +192,7 @@ static int upload_args(sclbm_batch *b, const std::vector<int> &ty)
     SCLBM_CUDA(cudaMalloc(&b->d_args, h.size() * sizeof(Fused2Args<S, T>)));
     SCLBM_CUDA(cudaMemcpy(b->d_args, h.data(), h.size() * sizeof(Fused2Args<S, T>),
                           cudaMemcpyHostToDevice));
-    return build_rings<S, T>(b, h, RING_BATCH_ROWS);
+    return build_rings<S, T>(b, h, ring_rows);
 }
 
 extern "C" {
@@ -230,6 +232,8 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
     b->parity = b->doms[0]->parity;
     std::vector<int> ty(ndomains);
     double nodes_units = 0.0, nodes_tiles = 0.0;
+    const SclbmTunedShape bd = tuned_batch_default(b->prec);
+    const bool bd_list = bd.variant == 2 || bd.variant == 8 || bd.variant == 9 || bd.variant == 10;
     for (int k = 0; k < ndomains; ++k) {
         sclbm_domain *d = b->doms[k];
         if (!d || d->ncomp != 2 || d->prec != b->prec || d->parity != b->parity) {
@@ -245,7 +249,8 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
         if (d->has_solid) b->flags |= KF_SOLID;
         if (d->p.force_on[0] || d->p.force_on[1]) b->flags |= KF_FORCE;
         const SclbmTunedShape ts = tuned_shape(d->nx, d->ny, b->prec);
-        ty[k] = tile_y_per_domain && tile_y_per_domain[k] > 0 ? tile_y_per_domain[k] : ts.tile_y;
+        ty[k] = tile_y_per_domain && tile_y_per_domain[k] > 0 ? tile_y_per_domain[k]
+                : (bd_list && bd.tile_y > 0 && d->has_solid ? bd.tile_y : ts.tile_y);
         (ts.variant == 3 ? nodes_units : nodes_tiles) += (double)d->nx * (double)d->ny;
     }
     // tile lists of tiles `width` columns wide, largest tiles first
@@ -285,10 +290,17 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
                                               : b->ntiles;
         b->grid_body[body] = std::max(1, std::min(units, pb * sm_count()));
     }
+    // rows per unit of the ring bodies: the caller's tile_y, else the tuned
+    // batch default's, else RING_BATCH_ROWS
+    std::vector<int> ring_rows(ndomains);
+    for (int k = 0; k < ndomains; ++k)
+        ring_rows[k] = tile_y_per_domain && tile_y_per_domain[k] > 0
+                           ? tile_y_per_domain[k]
+                           : ((bd.variant == 11 || bd.variant == 12) && bd.tile_y > 0 ? bd.tile_y : RING_BATCH_ROWS);
     switch (b->prec) {
-    case SCLBM_FP64: rc = upload_args<double, double>(b, ty); break;
-    case SCLBM_FP32_SHIFTED: rc = upload_args<float, float>(b, ty); break;
-    default: rc = upload_args<__half, float>(b, ty); break;
+    case SCLBM_FP64: rc = upload_args<double, double>(b, ty, ring_rows); break;
+    case SCLBM_FP32_SHIFTED: rc = upload_args<float, float>(b, ty, ring_rows); break;
+    default: rc = upload_args<__half, float>(b, ty, ring_rows); break;
     }
     // pipelined kernel: the smallest band height whose (domain, strip, band)
     // tiles all fit resident at once, bands of one domain split its rows evenly.
@@ -303,10 +315,27 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
                                                                    : BODY_UNIFORM;
     b->body = b->auto_body;
     b->use_units = b->auto_units;
-    // FP32/FP64 batches with solid nodes: the ring body on 128-column strips
-    // (512-domain ensemble: FP32 24.5 vs 21.3 GLUPS for the uniform tile list,
-    // FP64 12.0 vs 10.3; FP16 keeps its one-warp tile list, 24.9 vs 24.1)
-    b->auto_ring = b->ring && (b->flags & KF_SOLID) && b->prec != SCLBM_FP16_SHIFTED ? 128 : 0;
+    // Batches with solid nodes run the body that the autotuner's sweep of the
+    // whole mixed 512-domain ensemble found fastest for the precision (the
+    // tuned batch default); without one recorded, FP32/FP64 take the ring body
+    // on 128-column strips (ensemble: FP32 24.5 vs 21.3 GLUPS for the uniform
+    // tile list, FP64 12.0 vs 10.3) and FP16 its one-warp tile list.
+    if (b->flags & KF_SOLID) {
+        if ((bd.variant == 11 || bd.variant == 12) && b->ring) {
+            b->auto_ring = bd.variant == 11 ? 128 : 64;
+        } else if (bd.variant == 2 || bd.variant == 8 || bd.variant == 10 || bd.variant == 9) {
+            if (b->prec != SCLBM_FP64)
+                b->auto_body = bd.variant == 8 ? BODY_UNIFORM : bd.variant == 10 ? BODY_WARP
+                               : bd.variant == 9 ? BODY_HALF : BODY_TILE;
+            b->auto_units = 0;
+        } else if (bd.variant == 3 && b->prec != SCLBM_FP16_SHIFTED) {
+            b->auto_units = 1;
+        } else if (bd.variant == 0) {
+            b->auto_ring = b->ring && b->prec != SCLBM_FP16_SHIFTED ? 128 : 0;
+        }
+        b->body = b->auto_body;
+        b->use_units = b->auto_units;
+    }
     b->use_ring = b->auto_ring;
     std::vector<BandTile> bands;
     if (b->prec != SCLBM_FP16_SHIFTED) {

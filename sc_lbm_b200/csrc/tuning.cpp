@@ -9,6 +9,12 @@ static const SclbmTunedShape kDefault[3] = {{3, 16}, {2, 16}, {2, 32}};
 
 bool tuned_table_present() { return SCLBM_TUNED_COUNT > 0; }
 
+SclbmTunedShape tuned_batch_default(int precision)
+{
+    if (precision < 0 || precision > 2) return SclbmTunedShape{0, 0};
+    return kSclbmBatchDefault[precision];
+}
+
 SclbmTunedShape tuned_shape(size_t nx, size_t ny, int precision, int *recommended)
 {
     if (precision < 0 || precision > 2) precision = -1;

@@ -20,3 +20,8 @@ struct SclbmTunedClass {
 SclbmTunedShape tuned_shape(size_t nx, size_t ny, int precision, int *recommended = nullptr);
 /// Whether a measured table was compiled in
 bool tuned_table_present();
+/// Batch body for batches with solid nodes that the autotuner's sweep of the
+/// whole mixed ensemble found fastest for a storage precision: variant (11 or
+/// 12 the ring bodies, 2/8/10 tile lists, 3 bands; 0 = none recorded: the
+/// size-class table decides) and its rows per unit / tile (0 = default).
+SclbmTunedShape tuned_batch_default(int precision);

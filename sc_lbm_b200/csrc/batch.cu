@@ -253,6 +253,30 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
                 : (bd_list && bd.tile_y > 0 && d->has_solid ? bd.tile_y : ts.tile_y);
         (ts.variant == 3 ? nodes_units : nodes_tiles) += (double)d->nx * (double)d->ny;
     }
+    // Small batches: tiles as tall as the table's (tuned on batches of ~4M
+    // nodes) would leave most CTAs idle -- a batch of five 256^2 domains got 60
+    // tiles of 64 rows for 740 resident CTAs.  Heights the caller did not set
+    // are halved (down to 4 rows) until there are four tiles per resident CTA.
+    {
+        const long resident = (long)std::max(1, batch_blocks_per_sm(b->prec)) * sm_count();
+        auto count = [&]() {
+            long n = 0;
+            for (int k = 0; k < ndomains; ++k)
+                n += (long)((b->doms[k]->nx + BATCH_TX - 3) / (BATCH_TX - 2)) *
+                     (long)((b->doms[k]->ny + ty[k] - 1) / ty[k]);
+            return n;
+        };
+        const bool given = tile_y_per_domain != nullptr;
+        while (!given && count() < 4 * resident) {
+            bool changed = false;
+            for (int k = 0; k < ndomains; ++k)
+                if (ty[k] > 4) {
+                    ty[k] = std::max(4, ty[k] / 2);
+                    changed = true;
+                }
+            if (!changed) break;
+        }
+    }
     // tile lists of tiles `width` columns wide, largest tiles first
     auto tile_list = [&](int width) {
         const int w = width - 2;
@@ -297,6 +321,26 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
         ring_rows[k] = tile_y_per_domain && tile_y_per_domain[k] > 0
                            ? tile_y_per_domain[k]
                            : ((bd.variant == 11 || bd.variant == 12) && bd.tile_y > 0 ? bd.tile_y : RING_BATCH_ROWS);
+    if (!tile_y_per_domain) {
+        // as for the tile lists: four units per resident CTA, units of at least 8 rows
+        const long resident = (long)std::max(1, per_sm) * sm_count();
+        auto units = [&]() {
+            long n = 0;
+            for (int k = 0; k < ndomains; ++k)
+                n += (long)((b->doms[k]->nx + 127) / 128) *
+                     std::max(1L, (long)((b->doms[k]->ny + ring_rows[k] / 2) / ring_rows[k]));
+            return n;
+        };
+        while (units() < 4 * resident) {
+            bool changed = false;
+            for (int k = 0; k < ndomains; ++k)
+                if (ring_rows[k] > 8) {
+                    ring_rows[k] = std::max(8, ring_rows[k] / 2);
+                    changed = true;
+                }
+            if (!changed) break;
+        }
+    }
     switch (b->prec) {
     case SCLBM_FP64: rc = upload_args<double, double>(b, ty, ring_rows); break;
     case SCLBM_FP32_SHIFTED: rc = upload_args<float, float>(b, ty, ring_rows); break;

@@ -301,6 +301,18 @@ static bool ring_row_aligned(const sclbm_domain *d)
     return d->nx % (16 / elem_size(d->prec)) == 0;
 }
 
+// The ring's default 32-row bands give at least three waves of its resident
+// CTAs (four per SM for FP32 storage, three for FP64): on smaller lattices the
+// last partial wave costs more than the ring gains (2048 x 1024 FP64 porous:
+// 1.15 waves, 11.9 GLUPS against 14.2 for the register tile), and the
+// register tile, which sizes its tiles by the number of waves, is kept.
+static bool ring_fills_device(const sclbm_domain *d)
+{
+    const long per_sm = d->prec == SCLBM_FP64 ? 3 : 4;
+    const long units = (long)((d->nx + 127) / 128) * (long)((d->ny + 31) / 32);
+    return units >= 3 * per_sm * sm_count();
+}
+
 template <typename S, typename T>
 static cudaError_t step_one(const sclbm_domain *d, cudaStream_t s)
 {
@@ -344,7 +356,7 @@ static cudaError_t step_one(const sclbm_domain *d, cudaStream_t s)
     // force: FP32 0.498 ms with four stages against 0.542 for the uniform
     // register tile; FP64 0.955 with three against 1.061); all-fluid lattices
     // and FP16 storage keep the register tile, which is faster there
-    if (d->variant == 0 && d->has_solid && sizeof(S) != 2 && ring_row_aligned(d)) {
+    if (d->variant == 0 && d->has_solid && sizeof(S) != 2 && ring_row_aligned(d) && ring_fills_device(d)) {
         if constexpr (sizeof(S) == 8) return launch_ring2_fp64(a, 0, d->tile_y, s);
         else if constexpr (sizeof(S) == 4) return launch_ring2_f32(a, 1, d->tile_y, s);
     }

@@ -244,6 +244,20 @@ int sclbm_domain_download_f(sclbm_domain *d, int comp, double *f, size_t count);
  * no reference counterpart (the reference's perturbed init,
  * src/fluid.cpp:107-151, is unseeded). */
 int sclbm_domain_init_noise(sclbm_domain *d, int comp, double rho0, double amp, uint64_t seed);
+/* Seeded porous medium built on the device: the non-overlapping disks of
+ * sclbm_geometry_add_random_disks with the same arguments, placed against the
+ * domain's current mask (walls and earlier solids) and rasterised into it
+ * with the reference's integer circle (Geometry::add_circle,
+ * src/geometry.cpp:132-147; Ellipse::find_nodes,
+ * src/geom_object/ellipse.cpp:12-34): the resulting mask equals the host
+ * geometry's node for node.  Populations of the new solid nodes are zeroed.
+ * Call it before uploading or initialising populations.  Synchronises the
+ * library stream; *placed (may be NULL) = disks placed.  No reference
+ * counterpart (the reference's drivers place objects by hand). */
+int sclbm_domain_add_random_disks(sclbm_domain *d, double porosity, int rmin, int rmax, uint64_t seed,
+                                  int wall_rows, long max_tries, long max_misses, size_t *placed);
+/* The device mask (1 fluid, 0 solid; count must be nx*ny). */
+int sclbm_domain_download_mask(sclbm_domain *d, int32_t *mask, size_t count);
 /* density (Fluid::compute_density) and velocity (Fluid::compute_velocities) */
 int sclbm_domain_download_rho(sclbm_domain *d, int comp, double *rho, size_t count);
 int sclbm_domain_download_velocity(sclbm_domain *d, int comp, double *ux, double *uy,

@@ -261,6 +261,22 @@ class Domain(_Handle):
         v = np.ascontiguousarray(f, dtype=np.float64).ravel()
         call("sclbm_domain_upload_f", self._h, comp, _dp(v), v.size)
 
+    def add_random_disks(self, porosity, rmin, rmax, seed, wall_rows=0, max_tries=20000,
+                         max_misses=300) -> int:
+        """Seeded non-overlapping disks to the given fluid fraction, placed and
+        rasterised on the device; the same disks as Geometry.add_random_disks
+        with the same arguments on the same mask.  Returns the disks placed."""
+        n = C.c_size_t()
+        call("sclbm_domain_add_random_disks", self._h, float(porosity), int(rmin), int(rmax),
+             int(seed), int(wall_rows), int(max_tries), int(max_misses), C.byref(n))
+        return n.value
+
+    def download_mask(self) -> np.ndarray:
+        """The device mask (int32, 1 fluid, 0 solid)."""
+        m = np.zeros(self.N, np.int32)
+        call("sclbm_domain_download_mask", self._h, m.ctypes.data_as(C.POINTER(C.c_int32)), self.N)
+        return m
+
     def init_noise(self, comp, rho0, amp, seed):
         """f_i = rho/9, rho = rho0*(1 + amp*(2u-1)), u = splitmix64(seed, node),
         written on the device (equal to uploading workloads.populations)."""

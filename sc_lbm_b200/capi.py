@@ -109,6 +109,9 @@ SIGNATURES = {
     "sclbm_domain_upload_f": (C.c_int, [_VP, C.c_int, _D, _SZ]),
     "sclbm_domain_download_f": (C.c_int, [_VP, C.c_int, _D, _SZ]),
     "sclbm_domain_init_noise": (C.c_int, [_VP, C.c_int, C.c_double, C.c_double, C.c_uint64]),
+    "sclbm_domain_add_random_disks": (C.c_int, [_VP, C.c_double, C.c_int, C.c_int, C.c_uint64,
+                                                C.c_int, C.c_long, C.c_long, C.POINTER(_SZ)]),
+    "sclbm_domain_download_mask": (C.c_int, [_VP, C.POINTER(C.c_int32), _SZ]),
     "sclbm_domain_download_rho": (C.c_int, [_VP, C.c_int, _D, _SZ]),
     "sclbm_domain_download_velocity": (C.c_int, [_VP, C.c_int, _D, _D, _SZ]),
     "sclbm_domain_step": (C.c_int, [_VP, C.c_int]),

@@ -159,9 +159,9 @@ def spinodal(nx: int, ny: int, seed: int = 101, amp: float = 0.01):
                 f1=f[0], f2=f[1])
 
 
-def ensemble_member(k: int, seed: int = 2024, size=None):
-    """Domain k of the seeded ensemble (its own stream: members are
-    independent of how many are drawn)."""
+def ensemble_draws(k: int, seed: int = 2024, size=None) -> dict:
+    """The seeded draws of ensemble domain k: size, target fluid fraction,
+    G, Gs, tau, and the arguments of its disk packing."""
     s = Stream(seed * 100003 + k)
     if size is None:
         nx = 16 * s.integer(4, 32)
@@ -172,6 +172,16 @@ def ensemble_member(k: int, seed: int = 2024, size=None):
     G = s.uniform(0.8, 1.2)
     gs = s.uniform(-0.3, 0.3)
     tau = s.uniform(0.6, 1.5)
+    return dict(nx=nx, ny=ny, phi=phi, G=G, gs=gs, tau=tau,
+                disks=dict(porosity=phi, rmin=2, rmax=8, seed=seed * 7919 + k, wall_rows=0,
+                           max_tries=4000, max_misses=300))
+
+
+def ensemble_member(k: int, seed: int = 2024, size=None):
+    """Domain k of the seeded ensemble (its own stream: members are
+    independent of how many are drawn)."""
+    e = ensemble_draws(k, seed, size)
+    nx, ny, phi, G, gs, tau = e["nx"], e["ny"], e["phi"], e["G"], e["gs"], e["tau"]
     m, disks, phi_got = disk_mask(nx, ny, phi, 2, 8, seed * 7919 + k, max_tries=4000)
     N = nx * ny
     r1 = 1.0 + 0.01 * (2 * uniform(seed + 3 * k, N) - 1)

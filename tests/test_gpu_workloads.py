@@ -162,3 +162,48 @@ def test_unstable_ensemble_member_blows_up_with_the_reference(sclbm, k):
     d.step(1)
     with pytest.raises(capi.SclbmNonFinite):
         d.mass_momentum()
+
+
+def _packing_cases():
+    from sc_lbm_b200 import workloads as W
+    out = [dict(name="drainage_2048x1024", nx=2048, ny=1024, walls="x",
+                disks=dict(porosity=0.6, rmin=8, rmax=20, seed=11, wall_rows=1, max_tries=20000,
+                           max_misses=300)),
+           dict(name="small_disks_1024", nx=1024, ny=1024, walls=None,
+                disks=dict(porosity=0.72, rmin=2, rmax=8, seed=31337, wall_rows=0, max_tries=400000,
+                           max_misses=2000))]
+    for k in (0, 1, 3, 17, 100, 511):
+        e = W.ensemble_draws(k)
+        out.append(dict(name=f"ensemble_{k}_{e['nx']}x{e['ny']}", nx=e["nx"], ny=e["ny"], walls=None,
+                        disks=e["disks"]))
+    return out
+
+
+@pytest.mark.parametrize("case", _packing_cases(), ids=lambda c: c["name"])
+def test_device_packing_equals_host_packer(sclbm, case):
+    """Disks placed and rasterised on the device (sclbm_domain_add_random_disks)
+    give the host packer's mask node for node (Geometry.add_random_disks, the
+    reference's integer circle), the same number of disks, and zero
+    populations at the new solid nodes."""
+    nx, ny, dk = case["nx"], case["ny"], case["disks"]
+    g = sclbm.Geometry(nx, ny)
+    if case["walls"]:
+        g.add_walls(1, case["walls"])
+    base = g.get_geom().copy()
+    n_host = g.add_random_disks(**dk)
+    want = g.get_geom()
+    for prec in (sclbm.FP64, sclbm.FP32_SHIFTED):
+        d = sclbm.Domain(nx, ny, base, sclbm.make_params(ncomp=2, g_fluid=(0.9, 0.9)), prec)
+        d.init_noise(0, 1.0, 0.01, 5)
+        d.init_noise(1, 1.0, 0.01, 6)
+        n_dev = d.add_random_disks(**dk)
+        assert n_dev == n_host, (case["name"], n_dev, n_host)
+        got = d.download_mask()
+        assert np.array_equal(got, want), (case["name"], int(np.sum(got != want)))
+        solid = want == 0
+        for comp in range(2):
+            f = d.download_f(comp).reshape(9, -1)
+            if prec == sclbm.FP64:
+                assert np.all(f[:, solid] == 0.0)
+        d.step(3)
+        d.mass_momentum()

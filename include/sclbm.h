@@ -408,6 +408,28 @@ int sclbm_domain_contact_angle(sclbm_domain *d, int bulk, double rho_bulk, doubl
 size_t sclbm_domain_halo_bytes(const sclbm_domain *d, int rows);
 int sclbm_domain_halo_pack(sclbm_domain *d, int rows, int side, void *dst);
 int sclbm_domain_halo_unpack(sclbm_domain *d, int rows, int side, const void *src);
+/* Per-step exchange with one ghost row per side (the domain is the slab's
+ * owned rows plus one ghost row below and one above; exchange after every
+ * step): nine values per component and column per side instead of whole
+ * rows -- the six populations of the row next to the cut that the neighbour
+ * cannot compute itself, and the three that crossed the cut.  Owned rows stay
+ * bit-identical to one domain holding the whole lattice.  The buffer holds
+ * sclbm_domain_halo_min_bytes(d) bytes, [component][9][nx] of the storage
+ * type.  pack side 0 goes to the slab below (it unpacks it as side 1), side
+ * 1 to the slab above (unpacked as side 0).  The reference's MATLAB slab
+ * generator exchanges the crossing populations and a density row
+ * (tests/lbm/lbm_matlab/two_phase_flow/main_droplet.m:300-465); a density row
+ * instead of the six populations would change the order of the ghost
+ * density's sum and with it the last bits. */
+size_t sclbm_domain_halo_min_bytes(const sclbm_domain *d);
+int sclbm_domain_halo_min_pack(sclbm_domain *d, int side, void *dst);
+int sclbm_domain_halo_min_unpack(sclbm_domain *d, int side, const void *src);
+/* One step of the domain rows [row0, row0 + nrows) only (register tile, into
+ * the other buffer); finish = 1 ends the step (swaps the buffers) once every
+ * row has been stepped.  A slab steps the rows that need no halo (all but
+ * the three at each cut) while its exchange is in flight, then the rest.
+ * Two-component domains. */
+int sclbm_domain_step_rows(sclbm_domain *d, int row0, int nrows, int finish);
 
 /* ------------------------------------------------------------------- batch
  * Many independent domains of one precision advanced together: one launch

@@ -318,6 +318,20 @@ class Domain(_Handle):
     def halo_unpack(self, rows, side, ptr):
         call("sclbm_domain_halo_unpack", self._h, int(rows), int(side), C.c_void_p(int(ptr)))
 
+    # per-step exchange with one ghost row per side (slab.cu)
+    def halo_min_bytes(self) -> int:
+        return int(lib().sclbm_domain_halo_min_bytes(self._h))
+
+    def halo_min_pack(self, side, ptr):
+        call("sclbm_domain_halo_min_pack", self._h, int(side), C.c_void_p(int(ptr)))
+
+    def halo_min_unpack(self, side, ptr):
+        call("sclbm_domain_halo_min_unpack", self._h, int(side), C.c_void_p(int(ptr)))
+
+    def step_rows(self, row0, nrows, finish=False):
+        """One step of rows [row0, row0 + nrows); finish ends the step."""
+        call("sclbm_domain_step_rows", self._h, int(row0), int(nrows), 1 if finish else 0)
+
     def set_threads(self, tx):
         call("sclbm_domain_set_threads", self._h, int(tx))
 

@@ -142,6 +142,10 @@ SIGNATURES = {
     "sclbm_domain_halo_bytes": (_SZ, [_VP, C.c_int]),
     "sclbm_domain_halo_pack": (C.c_int, [_VP, C.c_int, C.c_int, _VP]),
     "sclbm_domain_halo_unpack": (C.c_int, [_VP, C.c_int, C.c_int, _VP]),
+    "sclbm_domain_halo_min_bytes": (_SZ, [_VP]),
+    "sclbm_domain_halo_min_pack": (C.c_int, [_VP, C.c_int, _VP]),
+    "sclbm_domain_halo_min_unpack": (C.c_int, [_VP, C.c_int, _VP]),
+    "sclbm_domain_step_rows": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int]),
     "sclbm_geometry_add_random_disks": (C.c_int, [_VP, C.c_double, C.c_int, C.c_int, C.c_uint64,
                                                   C.c_int, C.c_long, C.c_long,
                                                   C.POINTER(_SZ)]),

@@ -492,6 +492,54 @@ fail:
     return rc;
 }
 
+// One step of the rows [row0, row0 + nrows) only (register tile), into the
+// other buffer; `finish` ends the step (flips the buffers) once every row has
+// been stepped.  For overlapping a slab's halo exchange with the rows that do
+// not need it (sc_lbm_b200/slabs.py).
+int sclbm_domain_step_rows(sclbm_domain *d, int row0, int nrows, int finish)
+{
+    if (!d) return set_error(SCLBM_E_INVALID_ARGUMENT, "null domain");
+    if (d->ncomp != 2) return set_error(SCLBM_E_INVALID_ARGUMENT, "row ranges are for two-component domains");
+    if (row0 < 0 || nrows < 0 || (size_t)row0 + (size_t)nrows > d->ny)
+        return set_error(SCLBM_E_OUT_OF_RANGE, "row range outside the domain");
+    if (d->variant == 1) return set_error(SCLBM_E_INVALID_ARGUMENT, "row ranges need a single-pass variant");
+    cudaStream_t s = stream();
+    if (nrows > 0) {
+        // the register tile (in its uniform solid form for shifted lattices with solid nodes)
+        const int v = d->has_solid && d->prec != SCLBM_FP64 ? 8 : 2;
+        cudaError_t e;
+        switch (d->prec) {
+        case SCLBM_FP64: {
+            Fused2Args<double, double> a;
+            fill2(d, a);
+            a.row0 = row0;
+            a.row_end = row0 + nrows;
+            e = launch_fused2_fp64(a, v, 128, s);
+            break;
+        }
+        case SCLBM_FP32_SHIFTED: {
+            Fused2Args<float, float> a;
+            fill2(d, a);
+            a.row0 = row0;
+            a.row_end = row0 + nrows;
+            e = launch_fused2_f32(a, v, 128, s);
+            break;
+        }
+        default: {
+            Fused2Args<__half, float> a;
+            fill2(d, a);
+            a.row0 = row0;
+            a.row_end = row0 + nrows;
+            e = launch_fused2_f16(a, v, 128, s);
+            break;
+        }
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "row-range step");
+    }
+    if (finish) d->parity ^= 1;
+    return SCLBM_OK;
+}
+
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y)
 {
     if (!d) return set_error(SCLBM_E_INVALID_ARGUMENT, "null domain");

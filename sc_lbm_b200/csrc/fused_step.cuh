@@ -440,7 +440,7 @@ __device__ __forceinline__ void fused2_tile_ahead(const Fused2Args<S, T> &a, con
     const int t = threadIdx.x;
     const int nx = a.nx, ny = a.ny;
     const int ncol = min(W, nx - xb);
-    const int nrow = min(a.tile_y, ny - yb);
+    const int nrow = min(a.tile_y, (a.row_end > 0 ? a.row_end : ny) - yb);
     const bool active = t <= ncol + 1;
     const bool interior = t >= 1 && t <= ncol;
     const int x = wrap1(xb - 1 + t, nx);
@@ -559,7 +559,7 @@ __device__ __forceinline__ void fused2_tile_compact(const Fused2Args<S, T> &a, c
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int nx = a.nx, ny = a.ny;
     const int ncol = min(W, nx - xb);
-    const int nrow = min(a.tile_y, ny - yb);
+    const int nrow = min(a.tile_y, (a.row_end > 0 ? a.row_end : ny) - yb);
     const bool active = t <= ncol + 1;
     const bool interior = t >= 1 && t <= ncol;
     const int x = wrap1(xb - 1 + t, nx);
@@ -696,7 +696,7 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
     const int t = threadIdx.x & (TX - 1); // column of this thread in its tile
     const int nx = a.nx, ny = a.ny;
     const int ncol = min(W, nx - xb);
-    const int nrow = min(a.tile_y, ny - yb);
+    const int nrow = min(a.tile_y, (a.row_end > 0 ? a.row_end : ny) - yb);
     const bool active = t <= ncol + 1;
     const bool interior = t >= 1 && t <= ncol;
     const int x = wrap1(xb - 1 + t, nx);
@@ -813,12 +813,12 @@ __global__ void __launch_bounds__(TX, (fused_min_ctas<T, AHEAD, FLAGS, TX>()))
     __shared__ uint8_t s_m[4][TX];
     if constexpr (COMPACT && (FLAGS & KF_SOLID) != 0 && !TWO_PASS) {
         __shared__ CompactSmem<S, T, TX> cs;
-        fused2_tile_compact<S, T, TX, FLAGS>(a, blockIdx.x * (TX - 2), blockIdx.y * a.tile_y, s_rho,
-                                             s_m, cs, (blockIdx.y & 1) != 0);
+        fused2_tile_compact<S, T, TX, FLAGS>(a, blockIdx.x * (TX - 2), a.row0 + blockIdx.y * a.tile_y,
+                                             s_rho, s_m, cs, (blockIdx.y & 1) != 0);
     } else {
         fused2_tile<S, T, TX, TWO_PASS, FLAGS, PF, AHEAD, WIDE>(a, blockIdx.x * (TX - 2),
-                                                                blockIdx.y * a.tile_y, s_rho, s_m,
-                                                                (blockIdx.y & 1) != 0);
+                                                                a.row0 + blockIdx.y * a.tile_y, s_rho,
+                                                                s_m, (blockIdx.y & 1) != 0);
     }
 }
 
@@ -937,7 +937,8 @@ template <typename S, typename T, int TX, bool TWO, int FLAGS, bool PF = false, 
 inline cudaError_t launch_fused2_f(const Fused2Args<S, T> &a, cudaStream_t s)
 {
     constexpr int W = TX - 2;
-    const dim3 grid((a.nx + W - 1) / W, (a.ny + a.tile_y - 1) / a.tile_y);
+    const int rows = (a.row_end > 0 ? a.row_end : a.ny) - a.row0;
+    const dim3 grid((a.nx + W - 1) / W, (rows + a.tile_y - 1) / a.tile_y);
     k_fused2<S, T, TX, TWO, FLAGS, PF, AHEAD, COMPACT, WIDE><<<grid, TX, 0, s>>>(a);
     return cudaGetLastError();
 }

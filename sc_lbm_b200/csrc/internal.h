@@ -97,6 +97,8 @@ template <typename S, typename T> struct Fused2Args {
                                          // neither read nor write them (domain path)
     int *status;                         // set to 1 by a kernel whose bounded wait ran out
                                          // (ring kernel), or null
+    int row0, row_end;                   // register tile: step the rows [row0, row_end)
+                                         // only (row_end 0: up to ny)
 };
 
 // arguments of the single-component fused kernel

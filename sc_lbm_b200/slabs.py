@@ -16,11 +16,20 @@ main_droplet.m:162-465), which exchanges the three crossing populations and a
 density row per step; whole population rows keep the exchange a plain copy
 of contiguous rows and let k steps run between exchanges.
 
+Per-step mode (``per_step=True``): one ghost row per side, exchanged after
+every step, nine values per component and column per side -- the six
+populations of the row next to the cut that the neighbour cannot compute and
+the three that crossed the cut -- half of what the whole-row halo moves per
+step (18), still bit-identical.  Rows two or more away from a cut need nothing
+from the exchange, so ``run(..., overlap=True)`` steps them while the halo is
+in flight and the three rows at each cut afterwards (sclbm_domain_step_rows).
+A 4096-wide FP32 slab then exchanges 2 x 295 KB per step.
+
 Transports: ``LocalRing`` for slabs held by one process (device copies in
 stream order) and ``DistRing`` for one slab per rank (torch.distributed
-point-to-point: NCCL over NVLink between GPUs, gloo for host tensors).  The
-exchange is not overlapped with the step: the halo of a 4096-wide FP32 slab
-is 0.6 MB per side per exchange, about a microsecond on NVLink 5.
+point-to-point: NCCL over NVLink between GPUs, gloo for host tensors; NCCL
+runs on torch's stream, so the interior rows stepped on the library stream
+before it overlap with the transfer).
 """
 from __future__ import annotations
 
@@ -57,13 +66,14 @@ class Slab:
     upload_f / download_f methods, which the host-side tests use)."""
 
     def __init__(self, nx, ny, mask, y0, y1, halo_steps=1, make_domain=None, params=None,
-                 precision=None):
+                 precision=None, per_step=False):
         self.nx, self.ny, self.y0, self.y1 = int(nx), int(ny), int(y0), int(y1)
-        self.k = int(halo_steps)
-        self.H = 2 * self.k
+        self.per_step = bool(per_step)
+        self.k = 1 if self.per_step else int(halo_steps)
+        self.H = 1 if self.per_step else 2 * self.k
         if self.k < 1:
             raise ValueError("halo_steps >= 1")
-        if self.y1 - self.y0 < self.H:
+        if self.y1 - self.y0 < max(self.H, 1):
             raise ValueError("a slab needs at least 2 * halo_steps rows of its own")
         self.rows = np.arange(self.y0 - self.H, self.y1 + self.H) % self.ny
         m = np.asarray(mask, dtype=np.int32).reshape(self.ny, self.nx)[self.rows].ravel()
@@ -89,13 +99,35 @@ class Slab:
         return f[:, self.H:self.H + self.owned, :]
 
     def halo_bytes(self) -> int:
-        return self.domain.halo_bytes(self.H)
+        return self.domain.halo_min_bytes() if self.per_step else self.domain.halo_bytes(self.H)
 
     def pack(self, side: int, ptr: int) -> None:
-        self.domain.halo_pack(self.H, side, ptr)
+        if self.per_step:
+            self.domain.halo_min_pack(side, ptr)
+        else:
+            self.domain.halo_pack(self.H, side, ptr)
 
     def unpack(self, side: int, ptr: int) -> None:
-        self.domain.halo_unpack(self.H, side, ptr)
+        if self.per_step:
+            self.domain.halo_min_unpack(side, ptr)
+        else:
+            self.domain.halo_unpack(self.H, side, ptr)
+
+    # per-step mode: domain rows 0 and n-1 are the ghost rows; the exchange
+    # writes rows 0, 1, n-2 and n-1, and a row's step reads the densities of
+    # its neighbours, so rows [3, n-3) need nothing from it
+    def step_interior(self) -> None:
+        n = len(self.rows)
+        if n > 6:
+            self.domain.step_rows(3, n - 6, finish=False)
+
+    def step_boundary(self) -> None:
+        n = len(self.rows)
+        if n > 6:
+            self.domain.step_rows(0, 3, finish=False)
+            self.domain.step_rows(n - 3, 3, finish=True)
+        else:
+            self.domain.step_rows(0, n, finish=True)
 
 
 class LocalRing:
@@ -174,8 +206,22 @@ class DistRing:
         s.unpack(1, b["recv_up"].data_ptr())
 
 
-def run(slabs, transport, steps: int) -> None:
-    """Advance every slab `steps` steps, exchanging halos every k steps."""
+def run(slabs, transport, steps: int, overlap: bool = False) -> None:
+    """Advance every slab `steps` steps, exchanging halos every k steps.  In
+    per-step mode with `overlap`, each step runs the rows that need no halo,
+    then the exchange of the previous step's boundary values, then the rows
+    at the cuts (the exchange of the first step finds the state already
+    consistent and changes nothing); a last exchange completes the owned rows."""
+    if slabs[0].per_step and overlap:
+        for _ in range(int(steps)):
+            for s in slabs:
+                s.step_interior()
+            transport.exchange()
+            for s in slabs:
+                s.step_boundary()
+        if steps > 0:
+            transport.exchange()
+        return
     k = slabs[0].k
     left = int(steps)
     while left > 0:
@@ -195,6 +241,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--halo-steps", type=int, default=1)
     ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32", "fp16"])
+    ap.add_argument("--per-step", action="store_true",
+                    help="one ghost row, nine values per column and component per side every step, "
+                         "the exchange overlapped with the rows away from the cuts")
     args = ap.parse_args()
 
     import torch
@@ -216,17 +265,17 @@ def main():
     y0, y1 = partition(ny, world)[rank]
     params = sc.make_params(ncomp=2, g_fluid=(1.2, 1.2), rho_ref=(1.0, 1.0))
     slab = Slab(nx, ny, np.ones(nx * ny, np.int32), y0, y1, args.halo_steps, params=params,
-                precision=prec)
+                precision=prec, per_step=args.per_step)
     # spinodal-type state seeded on the device (per slab, not the global field)
     slab.domain.init_noise(0, 1.0, 0.01, 101 + 2 * rank)
     slab.domain.init_noise(1, 1.0, 0.01, 102 + 2 * rank)
     ring = DistRing(slab)
-    run([slab], ring, args.warmup)
+    run([slab], ring, args.warmup, overlap=args.per_step)
     dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    run([slab], ring, args.steps)
+    run([slab], ring, args.steps, overlap=args.per_step)
     e1.record()
     torch.cuda.synchronize()
     ms = torch.tensor([e0.elapsed_time(e1)], device="cuda")
@@ -235,6 +284,7 @@ def main():
     if rank == 0:
         print(json.dumps({"slabs": world, "lattice": [nx, ny], "precision": args.precision,
                           "halo_rows": slab.H, "halo_bytes_per_side": slab.halo_bytes(),
+                          "per_step": args.per_step,
                           "ms_per_step": round(ms_step, 5),
                           "mlups": round(nx * ny / (ms_step * 1e-3) / 1e6, 1)}))
     del ring, slab

@@ -59,6 +59,56 @@ def test_slabs_on_one_gpu_match_whole_lattice(sclbm, prec_name, k):
             assert s.owned_f(c).tobytes() == np.ascontiguousarray(w[:, y0:y1, :]).tobytes(), (y0, c)
 
 
+@pytest.mark.parametrize("prec_name", ["FP64", "FP32_SHIFTED", "FP16_SHIFTED"])
+@pytest.mark.parametrize("overlap", [False, True])
+def test_per_step_slabs_match_whole_lattice(sclbm, prec_name, overlap):
+    """One ghost row per side, nine values per component and column per side
+    each step (sclbm_domain_halo_min_*), with the rows away from the cuts
+    stepped before the exchange when `overlap` (sclbm_domain_step_rows): the
+    owned rows equal one domain holding the lattice, byte for byte."""
+    from sc_lbm_b200 import slabs
+    prec = getattr(sclbm, prec_name)
+    nx, ny, m, p, f1, f2 = _lattice(sclbm)
+    whole = sclbm.Domain(nx, ny, m, p, prec)
+    whole.upload_f(0, f1)
+    whole.upload_f(1, f2)
+    steps = 25
+    whole.step(steps)
+    cuts = [(0, 17), (17, 60), (60, 90)]
+    ss = [slabs.Slab(nx, ny, m, y0, y1, params=p, precision=prec, per_step=True) for y0, y1 in cuts]
+    es = {sclbm.FP64: 8, sclbm.FP32_SHIFTED: 4, sclbm.FP16_SHIFTED: 2}[prec]
+    assert ss[0].halo_bytes() == 2 * 9 * nx * es
+    for s in ss:
+        s.upload_f(0, f1)
+        s.upload_f(1, f2)
+    slabs.run(ss, slabs.LocalRing(ss), steps, overlap=overlap)
+    for c in range(2):
+        w = whole.download_f(c).reshape(9, ny, nx)
+        for s, (y0, y1) in zip(ss, cuts):
+            assert s.owned_f(c).tobytes() == np.ascontiguousarray(w[:, y0:y1, :]).tobytes(), \
+                (overlap, y0, c)
+
+
+def test_step_rows_in_pieces_equals_one_step(sclbm):
+    """Stepping a domain's rows in three pieces and finishing equals one step."""
+    nx, ny, m, p, f1, f2 = _lattice(sclbm)
+    for prec in (sclbm.FP64, sclbm.FP32_SHIFTED):
+        a = sclbm.Domain(nx, ny, m, p, prec)
+        b = sclbm.Domain(nx, ny, m, p, prec)
+        for d in (a, b):
+            d.upload_f(0, f1)
+            d.upload_f(1, f2)
+        a.step(2)
+        for _ in range(2):
+            b.step_rows(0, 31)
+            b.step_rows(60, 30)
+            b.step_rows(31, 29, finish=True)
+        for c in range(2):
+            assert a.download_f(c).tobytes() == b.download_f(c).tobytes()
+    with pytest.raises(IndexError):
+        b.step_rows(80, 20)
+
+
 def test_dist_ring_one_rank_nccl_on_the_library_stream(sclbm, tmp_path):
     """DistRing over an NCCL group of one rank while the library keeps its own
     stream (no set_stream): the exchange orders the library's copies and

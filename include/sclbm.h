@@ -268,8 +268,10 @@ int sclbm_domain_step(sclbm_domain *d, int nsteps);
  * FP64 (out[3*comp + 0..2]); out[6] = number of non-finite populations. */
 int sclbm_domain_mass_momentum(sclbm_domain *d, double out[7]);
 /* Kernel selection (all variants give identical results):
- *   0 = automatic (default): the fastest measured form -- 8 for FP32/FP16
- *       storage on lattices with solid nodes, 2 otherwise;
+ *   0 = automatic (default): the fastest measured form -- the ring kernel
+ *       (11; 12 for FP32) on FP32/FP64 lattices with solid nodes whose
+ *       32-row bands fill three waves of the GPU, else 8 for FP32/FP16
+ *       storage with solid nodes, 2 otherwise;
  *   1 = two pass (density kernel, then the fused kernel reading it);
  *   2 = single pass, one tile per CTA, population rows held in registers;
  *   3 = single pass, population rows staged through a shared-memory ring by
@@ -288,8 +290,15 @@ int sclbm_domain_mass_momentum(sclbm_domain *d, double out[7]);
  *       ones and storing zeros into their own slots (no branch around the
  *       collision; every slot written each step);
  *   9 = variant 3 with the solid form of variant 8 (FP64 and FP32 storage;
- *       FP16 runs variant 2).
- * tile_y = rows per tile of variants 1, 2 and 4-8 (0 keeps the default). */
+ *       FP16 runs variant 2);
+ *  11 = the ring kernel: 128-column strips x 32-row bands, population rows
+ *       streamed into a shared-memory ring by TMA tensor copies (one box of
+ *       nine directions per component and row) and collided from registers;
+ *       12 and 13 the same with one stage fewer / more.  Needs rows that
+ *       start on 16-byte boundaries (nx a multiple of 2, 4, 8 for FP64,
+ *       FP32, FP16); other lattices run variant 2.
+ * tile_y = rows per tile of variants 1, 2 and 4-8, rows per band of 11-13
+ * (0 keeps the default). */
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y);
 /* Threads per tile of the register-tile kernel (variants 1, 2, and 8 with
  * 32 or 128): 32 (one-warp tiles, no CTA barrier), 64 or 128. */
@@ -442,8 +451,15 @@ typedef struct sclbm_batch sclbm_batch;
 int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *tile_y_per_domain,
                        sclbm_batch **out);
 void sclbm_batch_destroy(sclbm_batch *b);
-/* Work decomposition (same results either way): 0 = automatic (the tuned
- * variant of the size class holding most of the batch's nodes); 2 = tile
+/* Work decomposition (same results either way): 0 = automatic (batches with
+ * solid nodes: the body the autotuner's mixed-ensemble sweep found fastest
+ * for the precision -- FP64/FP32 the ring body 11 with 16-row units, FP16
+ * the one-warp tile list 10; other batches: the tuned variant of the size
+ * class holding most of the batch's nodes); 11 = ring body: persistent CTAs
+ * take (domain, 128-column strip, band) units from a work counter and run
+ * the ring pipeline of domain variant 11 (rows per unit: tile_y_per_domain,
+ * else the tuned default); 12 = the same on 64-column strips (11, 12: every
+ * domain's rows on 16-byte boundaries); 2 = tile
  * list, tile_y rows per tile, register-tile body; 3 = 128-column strips x
  * row bands of one common height, pipelined body (FP64 and FP32 storage);
  * 5 = tile list with the load-ahead body, 6 = tile list with the compacted

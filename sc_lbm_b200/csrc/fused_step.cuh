@@ -206,6 +206,21 @@ __device__ __forceinline__ void push_one(const Fused2Args<S, T> &a, const int k,
     }
 }
 
+// The same push with the value already in the storage type (FP16: the
+// rounded value the mass closure used, stored without converting again).
+template <typename S, bool SOLID, bool WIDE = false, typename T>
+__device__ __forceinline__ void push_one_raw(const Fused2Args<S, T> &a, const int k, const int i,
+                                             const S v, const uint32_t nf, const Nbr &n)
+{
+    if (i == 0 || !SOLID) {
+        a.fout[k][elem<WIDE>(i, a.N, n.nb[i])] = v;
+    } else {
+        using O = Off<WIDE>;
+        const O to = elem<WIDE>(i, a.N, n.nb[i]), back = elem<WIDE>(opp(i), a.N, n.nb[0]);
+        a.fout[k][back ^ ((to ^ back) & (O(0) - O(nf)))] = v;
+    }
+}
+
 // Collide the node n.nb[0] from its populations f[k][i] (registers or shared
 // memory) and the density stencil, then push the results: the reference
 // sequence of src/lbm.cpp:177-204 (repulsive force), :250-269 (equilibrium
@@ -387,19 +402,43 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
             pair(2, 4, uy, uy45);                  // c = (0, +-1)
             pair(5, 7, ux + uy, ux45 + uy45);      // c = +-(1, 1)
             pair(6, 8, uy - ux, uy45 - ux45);      // c = +-(-1, 1)
+            if constexpr (sizeof(S) == 2) {
+                // FP16 storage: round each moving value once, store the half
+                // as it is and keep only its difference to the incoming value;
+                // the rest population closes the mass from those differences
+                // (the same sums, in the same order, as mass_closing_rest)
+                auto store_diff = [&](int i) -> float {
+                    float vi = v[i];
+                    if constexpr (FORCE) vi += a.c[k].force[i];
+                    __half h = __float2half_rn(vi);
+                    const float r = __half2float(h);
+                    if constexpr (UNIFORM) h = self_fluid ? h : __float2half_rn(0.f);
+                    push_one_raw<S, SOLID, WIDE>(a, k, i, h, nf[i], n);
+                    return float(f[k][i]) - r;
+                };
+                const float d1 = store_diff(1), d3 = store_diff(3);
+                const float d2 = store_diff(2), d4 = store_diff(4);
+                const float d5 = store_diff(5), d7 = store_diff(7);
+                const float d6 = store_diff(6), d8 = store_diff(8);
+                const float rest = float(f[k][0])
+                    + ((((d1 + d3) + (d2 + d4)) + ((d5 + d7) + (d6 + d8))) + (FORCE ? a.c[k].force_sum : 0.f));
+                __half h0 = __float2half_rn(rest);
+                if constexpr (UNIFORM) h0 = self_fluid ? h0 : __float2half_rn(0.f);
+                push_one_raw<S, SOLID, WIDE>(a, k, 0, h0, nf[0], n);
+            } else {
 #pragma unroll
-            for (int i = 1; i < 9; ++i) {
-                // the force vector is zero for a component without a volume force
-                if constexpr (FORCE) v[i] += a.c[k].force[i];
-                v[i] = stored_value<S>(v[i]);
-            }
-            // the rest population closes the node's mass (sum_i d*_i = sum_i d_i + sum_i F_i)
-            v[0] = mass_closing_rest(f[k], v, FORCE ? a.c[k].force_sum : 0.f);
+                for (int i = 1; i < 9; ++i) {
+                    // the force vector is zero for a component without a volume force
+                    if constexpr (FORCE) v[i] += a.c[k].force[i];
+                }
+                // the rest population closes the node's mass (sum_i d*_i = sum_i d_i + sum_i F_i)
+                v[0] = mass_closing_rest(f[k], v, FORCE ? a.c[k].force_sum : 0.f);
 #pragma unroll
-            for (int i = 0; i < 9; ++i) {
-                float vi = v[i];
-                if constexpr (UNIFORM) vi = self_fluid ? vi : 0.f;
-                push_one<S, T, SOLID, WIDE>(a, k, i, vi, nf[i], n);
+                for (int i = 0; i < 9; ++i) {
+                    float vi = v[i];
+                    if constexpr (UNIFORM) vi = self_fluid ? vi : 0.f;
+                    push_one<S, T, SOLID, WIDE>(a, k, i, vi, nf[i], n);
+                }
             }
         }
     }

@@ -281,6 +281,7 @@ static void fill2(const sclbm_domain *d, Fused2Args<S, T> &a)
         a.rho_in[k] = (const T *)d->rho_tmp[k];
         fill_comp<T>(a.c[k], d->p, k);
     }
+    pair_params(a.pc, a.c);
     a.solid_from_mask = 1;
     a.has_solid = d->has_solid ? 1 : 0;
     a.solids_zero = 1; // creation, uploads and initialisers write 0 at solid nodes

@@ -138,6 +138,31 @@ __device__ __forceinline__ float feq_dev(int i, float drho, float r, float ux, f
     return float(w_eq(i)) * fmaf(r, poly, drho);
 }
 
+// Packed FP32 pairs (sm_100 FFMA2 / FADD2 / FMUL2): in the float-arithmetic
+// collision x holds component 0 and y component 1.  Each lane rounds exactly
+// like the scalar operation (__fmaf_rn, __fadd_rn, __fmul_rn, a - b), so code
+// written on pairs gives the scalar sequence's results bit for bit with half
+// the arithmetic instructions.
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b)
+{
+    unsigned long long pa, pb, pd;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(pa) : "f"(a.x), "f"(a.y));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(pb) : "f"(b.x), "f"(b.y));
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(pd) : "l"(pa), "l"(pb));
+    float2 d;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(d.x), "=f"(d.y) : "l"(pd));
+    return d;
+}
+// one 64-bit read of a PairParams member
+__device__ __forceinline__ float2 pair_of(const float (&p)[2])
+{
+    return *reinterpret_cast<const float2 *>(p);
+}
+
 // The two components' densities of one node side by side, so a stencil read
 // fetches both with one 8- (16-) byte shared-memory load.
 template <typename T> struct Vec2;
@@ -331,115 +356,132 @@ __device__ __forceinline__ void collide_push(const Fused2Args<S, T> &a, const Po
         }
     } else {
         // shifted form: the stencil holds rho - rho_ref, and 0 at solid nodes, so
-        // the sums over fluid neighbours run over all neighbours without tests
-        float A0x = 0.f, A0y = 0.f, A1x = 0.f, A1y = 0.f, Sx = 0.f, Sy = 0.f;
+        // the sums over fluid neighbours run over all neighbours without tests.
+        // Both components advance side by side in packed pairs (x: component 0,
+        // y: component 1); every lane takes the scalar operation sequence.
+        const PairParams<T> &pc = a.pc;
+        // Ps.x = sum_i w c_i drho_0(nbr), Ps.y = sum_i w c_i drho_1(nbr)
+        float2 Psx = f2(0.f), Psy = f2(0.f);
+        float Sx = 0.f, Sy = 0.f;
 #pragma unroll
         for (int i = 1; i < 9; ++i) {
             const float wcx = float(w_sc(i) * cx(i)), wcy = float(w_sc(i) * cy(i));
-            if (cx(i)) { A0x = fmaf(wcx, p1[i], A0x); A1x = fmaf(wcx, p0[i], A1x); }
-            if (cy(i)) { A0y = fmaf(wcy, p1[i], A0y); A1y = fmaf(wcy, p0[i], A1y); }
+            const float2 q = make_float2(p0[i], p1[i]);
+            if (cx(i)) Psx = fma2(f2(wcx), q, Psx);
+            if (cy(i)) Psy = fma2(f2(wcy), q, Psy);
             if constexpr (SOLID) {
                 if (cx(i)) Sx += nf[i] ? 0.f : wcx;
                 if (cy(i)) Sy += nf[i] ? 0.f : wcy;
             }
         }
-        const float rr0 = a.c[0].rho_ref, rr1 = a.c[1].rho_ref;
-        const float r0 = rr0 + psi0, r1 = rr1 + psi1;
-        // sum over fluid neighbours of w c psi = A - rho_ref * S
-        float F0x, F0y, F1x, F1y;
+        const float2 RR = pair_of(pc.rho_ref);
+        const float2 DR = make_float2(psi0, psi1);
+        const float2 R = add2(RR, DR); // rho = rho_ref + drho
+        // each component feels the other's neighbours: sum over fluid
+        // neighbours of w c psi_other = Ps_other - rho_ref_other * S
+        float2 Ax = make_float2(Psx.y, Psx.x), Ay = make_float2(Psy.y, Psy.x);
         if constexpr (SOLID) {
-            F0x = a.c[0].gf * r0 * fmaf(-rr1, Sx, A0x);
-            F0y = a.c[0].gf * r0 * fmaf(-rr1, Sy, A0y);
-            F1x = a.c[1].gf * r1 * fmaf(-rr0, Sx, A1x);
-            F1y = a.c[1].gf * r1 * fmaf(-rr0, Sy, A1y);
-        } else {
-            F0x = a.c[0].gf * r0 * A0x;
-            F0y = a.c[0].gf * r0 * A0y;
-            F1x = a.c[1].gf * r1 * A1x;
-            F1y = a.c[1].gf * r1 * A1y;
+            const float2 nRR = make_float2(-RR.y, -RR.x);
+            Ax = fma2(nRR, f2(Sx), Ax);
+            Ay = fma2(nRR, f2(Sy), Ay);
         }
-        const T f01 = f[0][1], f03 = f[0][3], f05 = f[0][5], f06 = f[0][6], f07 = f[0][7], f08 = f[0][8];
-        const T f11 = f[1][1], f13 = f[1][3], f15 = f[1][5], f16 = f[1][6], f17 = f[1][7], f18 = f[1][8];
-        const float j0x = (f01 - f03) + (f05 - f06) + (f08 - f07);
-        const float j0y = (f[0][2] - f[0][4]) + (f05 + f06) - (f07 + f08);
-        const float j1x = (f11 - f13) + (f15 - f16) + (f18 - f17);
-        const float j1y = (f[1][2] - f[1][4]) + (f15 + f16) - (f17 + f18);
-        const float o0 = a.c[0].omega, o1 = a.c[1].omega;
-        const float inv_den = __fdividef(1.0f, fmaf(r0, o0, r1 * o1));
-        const float ucx = fmaf(j0x, o0, j1x * o1) * inv_den;
-        const float ucy = fmaf(j0y, o0, j1y * o1) * inv_den;
-        const float r[2] = {r0, r1}, dr[2] = {psi0, psi1};
-        const float Fx[2] = {F0x, F1x}, Fy[2] = {F0y, F1y};
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            float ux = ucx, uy = ucy;
-            if (!rho_is_zero(r[k])) {
-                const float io = a.c[k].inv_omega;
-                const float ir = io * __fdividef(1.0f, r[k]);
-                if constexpr (SOLID) {
-                    ux = fmaf(Fx[k], ir, fmaf(a.c[k].gs_neg * Sx, io, ucx));
-                    uy = fmaf(Fy[k], ir, fmaf(a.c[k].gs_neg * Sy, io, ucy));
-                } else {
-                    ux = fmaf(Fx[k], ir, ucx);
-                    uy = fmaf(Fy[k], ir, ucy);
-                }
-            }
-            // BGK toward the shifted equilibrium w_i (drho + rho poly_i),
-            // poly_i = 3 c.u + 4.5 (c.u)^2 - 1.5 u^2, written as
-            // d*_i = (1 - omega) d_i + w_i (omega rho poly_i + omega drho); the
-            // directions i and opp(i) share 4.5 (c.u)^2 - 1.5 u^2
-            const float usq15 = 1.5f * fmaf(ux, ux, uy * uy);
-            const float om = a.c[k].omega, omm = a.c[k].one_m_omega;
-            const float am = om * r[k], bm = om * dr[k];
-            const float ux45 = 4.5f * ux, uy45 = 4.5f * uy;
-            float v[9];
-            auto pair = [&](int i, int j, float cu, float cu45) {
-                const float sq = fmaf(cu45, cu, -usq15);
-                v[i] = fmaf(float(w_eq(i)), fmaf(am, fmaf(3.f, cu, sq), bm), omm * float(f[k][i]));
-                v[j] = fmaf(float(w_eq(j)), fmaf(am, fmaf(-3.f, cu, sq), bm), omm * float(f[k][j]));
-            };
-            pair(1, 3, ux, ux45);                  // c = (+-1, 0)
-            pair(2, 4, uy, uy45);                  // c = (0, +-1)
-            pair(5, 7, ux + uy, ux45 + uy45);      // c = +-(1, 1)
-            pair(6, 8, uy - ux, uy45 - ux45);      // c = +-(-1, 1)
+        const float2 G = mul2(pair_of(pc.gf), R);
+        const float2 Fx = mul2(G, Ax), Fy = mul2(G, Ay);
+        // direction i of both components
+        auto fp = [&](int i) { return make_float2(float(f[0][i]), float(f[1][i])); };
+        const float2 Jx = add2(add2(sub2(fp(1), fp(3)), sub2(fp(5), fp(6))), sub2(fp(8), fp(7)));
+        const float2 Jy = sub2(add2(sub2(fp(2), fp(4)), add2(fp(5), fp(6))), add2(fp(7), fp(8)));
+        const float2 OM = pair_of(pc.omega);
+        const float inv_den = __fdividef(1.0f, fmaf(R.x, OM.x, R.y * OM.y));
+        const float ucx = fmaf(Jx.x, OM.x, Jx.y * OM.y) * inv_den;
+        const float ucy = fmaf(Jy.x, OM.x, Jy.y * OM.y) * inv_den;
+        const float2 IO = pair_of(pc.inv_omega);
+        const float2 IR = mul2(IO, make_float2(__fdividef(1.0f, R.x), __fdividef(1.0f, R.y)));
+        float2 Ux, Uy;
+        if constexpr (SOLID) {
+            const float2 GS = pair_of(pc.gs_neg);
+            Ux = fma2(Fx, IR, fma2(mul2(GS, f2(Sx)), IO, f2(ucx)));
+            Uy = fma2(Fy, IR, fma2(mul2(GS, f2(Sy)), IO, f2(ucy)));
+        } else {
+            Ux = fma2(Fx, IR, f2(ucx));
+            Uy = fma2(Fy, IR, f2(ucy));
+        }
+        // a component of (numerically) zero density keeps the common velocity
+        if (rho_is_zero(R.x)) {
+            Ux.x = ucx;
+            Uy.x = ucy;
+        }
+        if (rho_is_zero(R.y)) {
+            Ux.y = ucx;
+            Uy.y = ucy;
+        }
+        // BGK toward the shifted equilibrium w_i (drho + rho poly_i),
+        // poly_i = 3 c.u + 4.5 (c.u)^2 - 1.5 u^2, written as
+        // d*_i = (1 - omega) d_i + w_i (omega rho poly_i + omega drho); the
+        // directions i and opp(i) share 4.5 (c.u)^2 - 1.5 u^2
+        const float2 NUSQ = mul2(f2(-1.5f), fma2(Ux, Ux, mul2(Uy, Uy))); // -1.5 u^2
+        const float2 OMM = pair_of(pc.one_m_omega);
+        const float2 AM = mul2(OM, R), BM = mul2(OM, DR);
+        const float2 Ux45 = mul2(f2(4.5f), Ux), Uy45 = mul2(f2(4.5f), Uy);
+        // Store direction i's post-collision pair (volume force added) and
+        // return d_i - d*_i as stored, the rest population's share
+        auto emit = [&](int i, float2 V) -> float2 {
+            if constexpr (FORCE) V = add2(V, pair_of(pc.force[i]));
             if constexpr (sizeof(S) == 2) {
-                // FP16 storage: round each moving value once, store the half
-                // as it is and keep only its difference to the incoming value;
-                // the rest population closes the mass from those differences
-                // (the same sums, in the same order, as mass_closing_rest)
-                auto store_diff = [&](int i) -> float {
-                    float vi = v[i];
-                    if constexpr (FORCE) vi += a.c[k].force[i];
-                    __half h = __float2half_rn(vi);
-                    const float r = __half2float(h);
-                    if constexpr (UNIFORM) h = self_fluid ? h : __float2half_rn(0.f);
-                    push_one_raw<S, SOLID, WIDE>(a, k, i, h, nf[i], n);
-                    return float(f[k][i]) - r;
-                };
-                const float d1 = store_diff(1), d3 = store_diff(3);
-                const float d2 = store_diff(2), d4 = store_diff(4);
-                const float d5 = store_diff(5), d7 = store_diff(7);
-                const float d6 = store_diff(6), d8 = store_diff(8);
-                const float rest = float(f[k][0])
-                    + ((((d1 + d3) + (d2 + d4)) + ((d5 + d7) + (d6 + d8))) + (FORCE ? a.c[k].force_sum : 0.f));
-                __half h0 = __float2half_rn(rest);
-                if constexpr (UNIFORM) h0 = self_fluid ? h0 : __float2half_rn(0.f);
-                push_one_raw<S, SOLID, WIDE>(a, k, 0, h0, nf[0], n);
+                // FP16: round once, store the halves as they are, close the
+                // mass with the rounded values
+                const __half2 H = __float22half2_rn(V);
+                __half h0 = __low2half(H), h1 = __high2half(H);
+                if constexpr (UNIFORM) {
+                    h0 = self_fluid ? h0 : __float2half_rn(0.f);
+                    h1 = self_fluid ? h1 : __float2half_rn(0.f);
+                }
+                push_one_raw<S, SOLID, WIDE>(a, 0, i, h0, nf[i], n);
+                push_one_raw<S, SOLID, WIDE>(a, 1, i, h1, nf[i], n);
+                return sub2(fp(i), __half22float2(H));
             } else {
-#pragma unroll
-                for (int i = 1; i < 9; ++i) {
-                    // the force vector is zero for a component without a volume force
-                    if constexpr (FORCE) v[i] += a.c[k].force[i];
+                float v0 = V.x, v1 = V.y;
+                if constexpr (UNIFORM) {
+                    v0 = self_fluid ? v0 : 0.f;
+                    v1 = self_fluid ? v1 : 0.f;
                 }
-                // the rest population closes the node's mass (sum_i d*_i = sum_i d_i + sum_i F_i)
-                v[0] = mass_closing_rest(f[k], v, FORCE ? a.c[k].force_sum : 0.f);
-#pragma unroll
-                for (int i = 0; i < 9; ++i) {
-                    float vi = v[i];
-                    if constexpr (UNIFORM) vi = self_fluid ? vi : 0.f;
-                    push_one<S, T, SOLID, WIDE>(a, k, i, vi, nf[i], n);
-                }
+                push_one<S, T, SOLID, WIDE>(a, 0, i, v0, nf[i], n);
+                push_one<S, T, SOLID, WIDE>(a, 1, i, v1, nf[i], n);
+                return sub2(fp(i), V);
             }
+        };
+        // directions i and j = opp(i) along cu; returns (d_i - d*_i) + (d_j - d*_j)
+        auto pair = [&](int i, int j, float2 CU, float2 CU45) -> float2 {
+            const float2 SQ = fma2(CU45, CU, NUSQ);
+            const float2 Vi = fma2(f2(float(w_eq(i))), fma2(AM, fma2(f2(3.f), CU, SQ), BM), mul2(OMM, fp(i)));
+            const float2 Vj = fma2(f2(float(w_eq(j))), fma2(AM, fma2(f2(-3.f), CU, SQ), BM), mul2(OMM, fp(j)));
+            const float2 Di = emit(i, Vi);
+            return add2(Di, emit(j, Vj));
+        };
+        const float2 D13 = pair(1, 3, Ux, Ux45);                            // c = (+-1, 0)
+        const float2 D24 = pair(2, 4, Uy, Uy45);                            // c = (0, +-1)
+        const float2 D57 = pair(5, 7, add2(Ux, Uy), add2(Ux45, Uy45));     // c = +-(1, 1)
+        const float2 D68 = pair(6, 8, sub2(Uy, Ux), sub2(Uy45, Ux45));     // c = +-(-1, 1)
+        // the rest population closes the node's mass (sum_i d*_i = sum_i d_i + sum_i F_i):
+        // d*_0 = d_0 + sum_{i>=1} (d_i - d*_i) [+ sum_i F_i]
+        const float2 FS = FORCE ? pair_of(pc.force_sum) : f2(0.f);
+        float2 V0 = add2(fp(0), add2(add2(add2(D13, D24), add2(D57, D68)), FS));
+        if constexpr (sizeof(S) == 2) {
+            const __half2 H = __float22half2_rn(V0);
+            __half h0 = __low2half(H), h1 = __high2half(H);
+            if constexpr (UNIFORM) {
+                h0 = self_fluid ? h0 : __float2half_rn(0.f);
+                h1 = self_fluid ? h1 : __float2half_rn(0.f);
+            }
+            push_one_raw<S, SOLID, WIDE>(a, 0, 0, h0, nf[0], n);
+            push_one_raw<S, SOLID, WIDE>(a, 1, 0, h1, nf[0], n);
+        } else {
+            if constexpr (UNIFORM) {
+                V0.x = self_fluid ? V0.x : 0.f;
+                V0.y = self_fluid ? V0.y : 0.f;
+            }
+            push_one<S, T, SOLID, WIDE>(a, 0, 0, V0.x, nf[0], n);
+            push_one<S, T, SOLID, WIDE>(a, 1, 0, V0.y, nf[0], n);
         }
     }
 }

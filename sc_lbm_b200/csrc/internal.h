@@ -80,6 +80,34 @@ template <typename T> struct CompParams {
     int force_on;
 };
 
+// The same constants of both components side by side (element 0: component
+// 0, element 1: component 1), each pair aligned so that one 64-bit read feeds
+// a packed FP32 instruction of the float-arithmetic collision.
+template <typename T> struct PairParams {
+    alignas(2 * sizeof(T)) T omega[2];
+    alignas(2 * sizeof(T)) T one_m_omega[2];
+    alignas(2 * sizeof(T)) T inv_omega[2];
+    alignas(2 * sizeof(T)) T gf[2];
+    alignas(2 * sizeof(T)) T gs_neg[2];
+    alignas(2 * sizeof(T)) T rho_ref[2];
+    alignas(2 * sizeof(T)) T force_sum[2];
+    alignas(2 * sizeof(T)) T force[9][2];
+};
+
+template <typename T> inline void pair_params(PairParams<T> &pc, const CompParams<T> (&c)[2])
+{
+    for (int k = 0; k < 2; ++k) {
+        pc.omega[k] = c[k].omega;
+        pc.one_m_omega[k] = c[k].one_m_omega;
+        pc.inv_omega[k] = c[k].inv_omega;
+        pc.gf[k] = c[k].gf;
+        pc.gs_neg[k] = c[k].gs_neg;
+        pc.rho_ref[k] = c[k].rho_ref;
+        pc.force_sum[k] = c[k].force_sum;
+        for (int i = 0; i < 9; ++i) pc.force[i][k] = c[k].force[i];
+    }
+}
+
 // arguments of the two-component fused kernel
 template <typename S, typename T> struct Fused2Args {
     int nx, ny, tile_y;
@@ -91,6 +119,7 @@ template <typename S, typename T> struct Fused2Args {
     const double *uex_old[2], *uey_old[2]; // kept u_eq for rho ~ 0 (FP64 path), or null
     const T *rho_in[2];                  // two-pass variant: density per node
     CompParams<T> c[2];
+    PairParams<T> pc;                    // c[0], c[1] side by side (filled with c)
     int solid_from_mask;                 // derive Fs from the mask (domain path)
     int has_solid;                       // the mask has solid nodes (else all fluid)
     int solids_zero;                     // both buffers hold 0 at solid nodes: the kernels

@@ -269,9 +269,11 @@ int sclbm_domain_step(sclbm_domain *d, int nsteps);
 int sclbm_domain_mass_momentum(sclbm_domain *d, double out[7]);
 /* Kernel selection (all variants give identical results):
  *   0 = automatic (default): the fastest measured form -- the ring kernel
- *       (11; 12 for FP32) on FP32/FP64 lattices with solid nodes whose
- *       32-row bands fill three waves of the GPU, else 8 for FP32/FP16
- *       storage with solid nodes, 2 otherwise;
+ *       on lattices whose rows start on 16-byte boundaries and whose bands
+ *       fill three waves of the GPU (FP64: the depth of 12 and 16-row bands;
+ *       FP32: the depth of 13 and 24-row bands; FP16: the depth of 12 and
+ *       32-row bands), else 8 for FP32/FP16 storage with solid nodes, 2
+ *       otherwise;
  *   1 = two pass (density kernel, then the fused kernel reading it);
  *   2 = single pass, one tile per CTA, population rows held in registers;
  *   3 = single pass, population rows staged through a shared-memory ring by

@@ -302,15 +302,34 @@ static bool ring_row_aligned(const sclbm_domain *d)
     return d->nx % (16 / elem_size(d->prec)) == 0;
 }
 
-// The ring's default 32-row bands give at least three waves of its resident
-// CTAs (four per SM for FP32 storage, three for FP64): on smaller lattices the
-// last partial wave costs more than the ring gains (2048 x 1024 FP64 porous:
-// 1.15 waves, 11.9 GLUPS against 14.2 for the register tile), and the
-// register tile, which sizes its tiles by the number of waves, is kept.
+// Ring depth (stages: -1, 0, +1 = the depths of variants 12, 11, 13) and rows
+// per band that variant 0 runs, the fastest measured on B200 at 4096 x 4096
+// (GLUPS all-fluid / 72 % fluid):
+//   FP64  2 stages, 16 rows: 20.3 / 15.3 (3 stages 19.8 / 14.9; register tile 18.5)
+//   FP32  4 stages, 24 rows: 41.6 (16 rows 41.3, 32 rows 40.1; 3 stages 36.8;
+//         5 stages 37.5; register tile 37.6) / 33.1 at 16 rows, 32.9 at 32
+//   FP16  4 stages, 32 rows: 49.4 / 35.6 (5 stages 49.0 / 35.3; register tile
+//         47.6 / 35.2)
+struct RingChoice {
+    int stages, rows;
+};
+static RingChoice ring_choice(const sclbm_domain *d)
+{
+    if (d->prec == SCLBM_FP64) return {-1, 16};
+    if (d->prec == SCLBM_FP32_SHIFTED) return {1, 24};
+    return {-1, 32};
+}
+
+// The ring's bands give at least three waves of its resident CTAs (four per
+// SM for FP32/FP16 storage, three for FP64): on smaller lattices the last
+// partial wave costs more than the ring gains (2048 x 1024 FP64 porous: 1.15
+// waves, 11.9 GLUPS against 14.2 for the register tile), and the register
+// tile, which sizes its tiles by the number of waves, is kept.
 static bool ring_fills_device(const sclbm_domain *d)
 {
     const long per_sm = d->prec == SCLBM_FP64 ? 3 : 4;
-    const long units = (long)((d->nx + 127) / 128) * (long)((d->ny + 31) / 32);
+    const long rows = d->tile_y > 0 ? d->tile_y : ring_choice(d).rows;
+    const long units = (long)((d->nx + 127) / 128) * (long)((d->ny + rows - 1) / rows);
     return units >= 3 * per_sm * sm_count();
 }
 
@@ -345,21 +364,19 @@ static cudaError_t step_one(const sclbm_domain *d, cudaStream_t s)
                                    (float *)d->rho_tmp[1], d->N, s);
         if (e != cudaSuccess) return e;
     }
-    // variant 0 picks the fastest measured form on B200: the register tile,
-    // with the uniform solid form where FP32/FP16 lattices have solid nodes
-    // (FP64 at 4096^2: register tile 17.4 GLUPS all-fluid, 15.4 at 60 % fluid,
-    // against 16.4 and 14.8 for the pipelined kernel); 3 and 9 force the
-    // pipelined kernel
-    // 11, 12, 13: the ring kernel (rows streamed into shared memory by tensor
-    // copies) with its default, fewer and more stages; lattices whose rows do
-    // not start on 16-byte boundaries take the register tile.  Variant 0 runs
-    // it on FP32 and FP64 lattices with solid nodes (4096^2, 60 % fluid, with
-    // force: FP32 0.498 ms with four stages against 0.542 for the uniform
-    // register tile; FP64 0.955 with three against 1.061); all-fluid lattices
-    // and FP16 storage keep the register tile, which is faster there
-    if (d->variant == 0 && d->has_solid && sizeof(S) != 2 && ring_row_aligned(d) && ring_fills_device(d)) {
-        if constexpr (sizeof(S) == 8) return launch_ring2_fp64(a, 0, d->tile_y, s);
-        else if constexpr (sizeof(S) == 4) return launch_ring2_f32(a, 1, d->tile_y, s);
+    // variant 0 picks the fastest measured form on B200: the ring kernel
+    // (rows streamed into shared memory by tensor copies) at the depth and
+    // band height of ring_choice on lattices whose rows start on 16-byte
+    // boundaries and whose bands fill three waves; else the register tile,
+    // in its uniform solid form where FP32/FP16 lattices have solid nodes.
+    // 3 and 9 force the pipelined kernel; 11, 12, 13 the ring kernel with its
+    // default, fewer and more stages (unaligned lattices: the register tile)
+    if (d->variant == 0 && ring_row_aligned(d) && ring_fills_device(d)) {
+        const RingChoice rc = ring_choice(d);
+        const int rows = d->tile_y > 0 ? d->tile_y : rc.rows;
+        if constexpr (sizeof(S) == 8) return launch_ring2_fp64(a, rc.stages, rows, s);
+        else if constexpr (sizeof(S) == 4) return launch_ring2_f32(a, rc.stages, rows, s);
+        else return launch_ring2_f16(a, rc.stages, rows, s);
     }
     if (d->variant >= 11 && d->variant <= 13 && ring_row_aligned(d)) {
         const int st = d->variant == 11 ? 0 : (d->variant == 12 ? -1 : 1);

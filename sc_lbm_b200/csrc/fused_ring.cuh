@@ -187,10 +187,13 @@ __device__ __forceinline__ bool ring_unit(const Fused2Args<S, T> &a, const CUten
     const int nx = a.nx, ny = a.ny;
     const int ncol = min(W, nx - xb);
     const bool act = t < ncol;
-    const bool hl = t == 0, hr = t == ncol - 1;
     const int x = act ? xb + t : xb;
     const int xl = wrap1(x - 1, nx), xr = wrap1(x + 1, nx);
-    const int xhl = wrap1(xb - 1, nx), xhr = wrap1(xb + ncol, nx);
+    // the densities of the two halo columns come from lanes 0 (left) and 1
+    // (right) of warp 0, which run the same instructions side by side (ncol >= 2:
+    // rows hold a multiple of A >= 2 nodes)
+    const bool hl = t == 0, hal = t <= 1;
+    const int xh = hl ? wrap1(xb - 1, nx) : wrap1(xb + ncol, nx);
     const int last = nrow + 1;
     const uint32_t gbase = g0;
     // lattice row of ring row j (tile row -1 .. nrow in march order)
@@ -241,12 +244,11 @@ __device__ __forceinline__ bool ring_unit(const Fused2Args<S, T> &a, const CUten
         }
 
     // masks of the next row, loaded one row ahead
-    uint8_t mn = 1, mnl = 1, mnr = 1;
+    uint8_t mn = 1, mnh = 1;
     if (SOLID && act) {
         const size_t row = (size_t)gy(0) * (size_t)nx;
         mn = a.mask[row + x];
-        if (hl) mnl = a.mask[row + xhl];
-        if (hr) mnr = a.mask[row + xhr];
+        if (hal) mnh = a.mask[row + xh];
     }
     bool aborted = false;
     int consumed = -1;
@@ -255,12 +257,11 @@ __device__ __forceinline__ bool ring_unit(const Fused2Args<S, T> &a, const CUten
     // into the ring; barrier; the stage is free, so request row j + R into it;
     // collide row j - 1 (prev) from the stencil rows j - 2, j - 1, j
     auto step_row = [&](const int j, T(&cur)[2][9], const T(&prev)[2][9]) {
-        const uint8_t m = mn, ml = mnl, mr = mnr;
+        const uint8_t m = mn, mh = mnh;
         if (SOLID && act && j < last) {
             const size_t row = (size_t)gy(j + 1) * (size_t)nx;
             mn = a.mask[row + x];
-            if (hl) mnl = a.mask[row + xhl];
-            if (hr) mnr = a.mask[row + xhr];
+            if (hal) mnh = a.mask[row + xh];
         }
         const int slot = j & 3;
         if (!aborted) {
@@ -272,13 +273,7 @@ __device__ __forceinline__ bool ring_unit(const Fused2Args<S, T> &a, const CUten
                 const S *hrp = reinterpret_cast<const S *>(sg + 2 * L::comp + 2 * L::halo);
                 auto density = [&](const T(&f)[2][9], uint8_t mm, int q) {
                     T r[2];
-#pragma unroll
-                    for (int k = 0; k < 2; ++k) {
-                        T s = T(0); // 0.0 + f0 + ... + f8, src/fluid.cpp:177-181
-#pragma unroll
-                        for (int i = 0; i < 9; ++i) s += f[k][i];
-                        r[k] = s;
-                    }
+                    node_density(f, r[0], r[1]);
                     if (SOLID && !mm) r[0] = r[1] = T(0);
                     rho[slot * Q + q] = Vec2<T>::make(r[0], r[1]);
                     msk[slot * Q + q] = SOLID ? mm : 1;
@@ -294,18 +289,17 @@ __device__ __forceinline__ bool ring_unit(const Fused2Args<S, T> &a, const CUten
                 if (act) {
                     load(stg, CE, P, A + t, cur);
                     density(cur, m, t + 1);
-                    if (hl || hr) {
+                    if (hal) {
+                        // the halo column wrapped around a lattice edge comes
+                        // from its own box, else from the row box
+                        const bool wrap = hl ? wrap_l : wrap_r;
+                        const S *hp = wrap ? (hl ? hlp : hrp) : stg;
+                        const uint32_t hcs = wrap ? HE : CE;
+                        const int hds = wrap ? A : P;
+                        const int hcol = wrap ? (hl ? A - 1 : 0) : (hl ? A - 1 : A + ncol);
                         T h[2][9];
-                        if (hl) {
-                            if (wrap_l) load(hlp, HE, A, A - 1, h);
-                            else load(stg, CE, P, A - 1, h);
-                            density(h, ml, 0);
-                        }
-                        if (hr) {
-                            if (wrap_r) load(hrp, HE, A, 0, h);
-                            else load(stg, CE, P, A + ncol, h);
-                            density(h, mr, ncol + 1);
-                        }
+                        load(hp, hcs, hds, hcol, h);
+                        density(h, mh, hl ? 0 : ncol + 1);
                     }
                 }
             } else {

@@ -163,6 +163,28 @@ __device__ __forceinline__ float2 pair_of(const float (&p)[2])
     return *reinterpret_cast<const float2 *>(p);
 }
 
+// Both components' densities of one node, 0.0 + f_0 + ... + f_8 in that
+// order (src/fluid.cpp:177-181); float arithmetic on packed pairs
+template <typename T> __device__ __forceinline__ void node_density(const T (&f)[2][9], T &r0, T &r1)
+{
+    if constexpr (sizeof(T) == 4) {
+        float2 s = f2(0.f);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) s = add2(s, make_float2(f[0][i], f[1][i]));
+        r0 = s.x;
+        r1 = s.y;
+    } else {
+        T s0 = T(0), s1 = T(0);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            s0 += f[0][i];
+            s1 += f[1][i];
+        }
+        r0 = s0;
+        r1 = s1;
+    }
+}
+
 // The two components' densities of one node side by side, so a stencil read
 // fetches both with one 8- (16-) byte shared-memory load.
 template <typename T> struct Vec2;
@@ -562,13 +584,7 @@ __device__ __forceinline__ void fused2_tile_ahead(const Fused2Args<S, T> &a, con
         T rho[2] = {T(0), T(0)};
         uint8_t m = 0;
         if (active) {
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                T s = T(0); // 0.0 + f0 + ... + f8, src/fluid.cpp:177-181
-#pragma unroll
-                for (int i = 0; i < 9; ++i) s += D[k][i];
-                rho[k] = s;
-            }
+            node_density(D, rho[0], rho[1]);
             m = SOLID ? mr : 1;
             if (SOLID && !m) rho[0] = rho[1] = T(0);
         }
@@ -673,13 +689,8 @@ __device__ __forceinline__ void fused2_tile_compact(const Fused2Args<S, T> &a, c
                     for (int i = 0; i < 9; ++i)
                         cur[k][i] = T(Store<S>::ld(a.fin[k] + elem<false>(i, a.N, node)));
             }
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                T sum = T(0); // 0.0 + f0 + ... + f8, src/fluid.cpp:177-181
-#pragma unroll
-                for (int i = 0; i < 9; ++i) sum += cur[k][i];
-                rho[k] = m ? sum : T(0);
-            }
+            node_density(cur, rho[0], rho[1]);
+            if (!m) rho[0] = rho[1] = T(0);
             if (!m && interior && !a.solids_zero && r >= 0 && r < nrow) {
                 // caller-owned arrays: the reference's stream leaves zeros at solids
 #pragma unroll
@@ -833,13 +844,7 @@ __device__ __forceinline__ void fused2_tile(const Fused2Args<S, T> &a, const int
                 rho[0] = a.rho_in[0][node];
                 rho[1] = a.rho_in[1][node];
             } else {
-#pragma unroll
-                for (int k = 0; k < 2; ++k) {
-                    T s = T(0); // 0.0 + f0 + ... + f8, src/fluid.cpp:177-181
-#pragma unroll
-                    for (int i = 0; i < 9; ++i) s += cur[k][i];
-                    rho[k] = s;
-                }
+                node_density(cur, rho[0], rho[1]);
             }
             if (SOLID && !m) rho[0] = rho[1] = T(0);
         } else {

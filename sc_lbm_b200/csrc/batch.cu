@@ -128,9 +128,18 @@ static int build_ring(sclbm_batch *b, const std::vector<Fused2Args<S, T>> &h, co
             }
         }
     }
+    // Largest first at domain granularity: a domain's units stay together in
+    // band-major order, so vertically neighbouring bands (opposite march
+    // directions) start within a few claims of each other and the halo rows
+    // they share are read from L2 the second time; domains are ordered by
+    // their largest unit.
+    std::vector<long> dom_cost(b->doms.size(), 0);
+    for (size_t i = 0; i < units.size(); ++i)
+        dom_cost[units[i].dom] = std::max(dom_cost[units[i].dom], cost[i]);
     std::vector<int> order(units.size());
     std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return cost[a] > cost[c]; });
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int c) { return dom_cost[units[a].dom] > dom_cost[units[c].dom]; });
     std::vector<RingUnit> sorted(units.size());
     for (size_t i = 0; i < order.size(); ++i) sorted[i] = units[order[i]];
     std::vector<RingMaps> maps(h.size());

@@ -235,6 +235,35 @@ def test_ring_kernel_ragged_lattices(sclbm, oracle, nx, ny, geom):
         b["_domain"].mass_momentum()
 
 
+@pytest.mark.parametrize("prec_name,ny,porous", [("FP64", 1024, False), ("FP32_SHIFTED", 1536, False),
+                                                 ("FP32_SHIFTED", 1536, True), ("FP16_SHIFTED", 2048, False)])
+def test_default_kernel_on_lattices_that_fill_the_gpu(sclbm, prec_name, ny, porous):
+    """Lattices large enough for the default kernel choice to take the ring
+    (4096 wide, 2048 bands of the precision's default height: 16 rows FP64, 24
+    FP32, 32 FP16) give the register tile's populations byte for byte after
+    three steps, all-fluid and porous with a volume force."""
+    from sc_lbm_b200 import workloads as W
+    prec = getattr(sclbm, prec_name)
+    nx = 4096
+    if porous:
+        mask, _, _ = W.disk_mask(nx, ny, 0.7, 4, 12, 17, walls="x")
+    else:
+        mask = np.ones(nx * ny, np.int32)
+    params = sclbm.make_params(ncomp=2, tau=(0.9, 1.1), g_fluid=(1.2, 1.2), g_solid=(-0.2, 0.2),
+                               rho_ref=(1.0, 1.0), force=(cases.force_vec(1e-5, "x") if porous else None, None))
+    digests = []
+    for variant in (0, 2):
+        d = sclbm.Domain(nx, ny, mask, params, prec)
+        d.set_kernel(variant, 0)
+        d.init_noise(0, 1.0, 0.02, 5)
+        d.init_noise(1, 1.0, 0.02, 6)
+        d.step(3)
+        d.mass_momentum()  # finite, no bounded wait ran out
+        digests.append([hashlib.sha256(d.download_f(k).tobytes()).hexdigest() for k in range(2)])
+        del d
+    assert digests[0] == digests[1], (prec_name, ny, porous)
+
+
 # ------------------------------------------------------------------- monitors
 def test_mass_momentum_monitor(sclbm):
     for prec in (sclbm.FP64, sclbm.FP32_SHIFTED, sclbm.FP16_SHIFTED):

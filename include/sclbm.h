@@ -455,11 +455,12 @@ int sclbm_batch_create(sclbm_domain *const *domains, int ndomains, const int *ti
 void sclbm_batch_destroy(sclbm_batch *b);
 /* Work decomposition (same results either way): 0 = automatic (batches with
  * solid nodes: the body the autotuner's mixed-ensemble sweep found fastest
- * for the precision -- FP64/FP32 the ring body 11 with 16-row units, FP16
- * the one-warp tile list 10; other batches: the tuned variant of the size
+ * for the precision -- the ring body 11 with 16-row units for FP64, 24 for
+ * FP32 and 32 for FP16; other batches: the tuned variant of the size
  * class holding most of the batch's nodes); 11 = ring body: persistent CTAs
- * take (domain, 128-column strip, band) units from a work counter and run
- * the ring pipeline of domain variant 11 (rows per unit: tile_y_per_domain,
+ * take (domain, 128-column strip, band) units from a work counter (each
+ * domain's units together, domains largest first) and run the ring pipeline
+ * of domain variant 11 (rows per unit: tile_y_per_domain,
  * else the tuned default); 12 = the same on 64-column strips (11, 12: every
  * domain's rows on 16-byte boundaries); 2 = tile
  * list, tile_y rows per tile, register-tile body; 3 = 128-column strips x

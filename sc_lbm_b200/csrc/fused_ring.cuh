@@ -14,9 +14,9 @@
 // engine's per-copy cost dominated at 300-1000 bytes a copy).
 //
 // Work decomposition.  A CTA of RING_W threads owns a strip of RING_W interior
-// columns and a band of rows (32 by default: several waves of CTAs, which the
-// block scheduler balances where bands hold different numbers of fluid
-// nodes).  Neighbouring bands march in opposite directions, so the two halo
+// columns and a band of rows (16 to 32 as the caller chooses: several waves
+// of CTAs, which the block scheduler balances where bands hold different
+// numbers of fluid nodes).  Neighbouring bands march in opposite directions, so the two halo
 // rows that a pair of bands shares are read by both near the same time and
 // the second read often hits L2.
 //
@@ -437,12 +437,12 @@ inline cudaError_t ring_maps(const Fused2Args<S, T> &a, RingMaps &m)
     return cudaSuccess;
 }
 
-// rows: rows per band (0: RING_ROWS).  Bands of 32 rows give 4096^2 lattices
-// about four waves of CTAs, which lets the block scheduler even out bands
-// whose fluid nodes, and so whose work, differ: on porous 4096^2 lattices one
-// wave of tall bands ran 5-25 % slower than 32-row bands, 128-row bands
-// 3-14 % slower (FP32 and FP64, disks of radius 8-20 at 60 % fluid and 2-8
-// at 72 %).
+// rows: rows per band (0: RING_ROWS; the domain's default choice passes its
+// own per-precision height).  Short bands give 4096^2 lattices several waves
+// of CTAs, which lets the block scheduler even out bands whose fluid nodes,
+// and so whose work, differ: on porous 4096^2 lattices one wave of tall bands
+// ran 5-25 % slower than 32-row bands, 128-row bands 3-14 % slower (FP32 and
+// FP64, disks of radius 8-20 at 60 % fluid and 2-8 at 72 %).
 constexpr int RING_ROWS = 32;
 template <typename S, typename T, int FLAGS, int R, bool WIDE>
 inline cudaError_t launch_ring2_f(const Fused2Args<S, T> &a, int rows, cudaStream_t s)

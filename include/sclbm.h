@@ -299,7 +299,12 @@ int sclbm_domain_mass_momentum(sclbm_domain *d, double out[7]);
  *       12 and 13 the same with one stage fewer / more.  Needs rows that
  *       start on 16-byte boundaries (nx a multiple of 2, 4, 8 for FP64,
  *       FP32, FP16); other lattices run variant 2.
- * tile_y = rows per tile of variants 1, 2 and 4-8, rows per band of 11-13
+ *  14 = FP32 storage: the ring kernel at the default depth and band height
+ *       without the halo boxes in each stage (the wrapped halo column of a
+ *       strip at the lattice edge is copied from global memory one row ahead
+ *       by asynchronous element copies), which makes room for five resident
+ *       CTAs per SM instead of four; FP64 and FP16 run their default ring.
+ * tile_y = rows per tile of variants 1, 2 and 4-8, rows per band of 11-14
  * (0 keeps the default). */
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y);
 /* Threads per tile of the register-tile kernel (variants 1, 2, and 8 with

@@ -378,6 +378,14 @@ static cudaError_t step_one(const sclbm_domain *d, cudaStream_t s)
         else if constexpr (sizeof(S) == 4) return launch_ring2_f32(a, rc.stages, rows, s);
         else return launch_ring2_f16(a, rc.stages, rows, s);
     }
+    if (d->variant == 14 && ring_row_aligned(d)) {
+        // the default depth without halo boxes in the stages
+        const RingChoice rc = ring_choice(d);
+        const int rows = d->tile_y > 0 ? d->tile_y : rc.rows;
+        if constexpr (sizeof(S) == 8) return launch_ring2_fp64(a, rc.stages, rows, s, true);
+        else if constexpr (sizeof(S) == 4) return launch_ring2_f32(a, rc.stages, rows, s, true);
+        else return launch_ring2_f16(a, rc.stages, rows, s, true);
+    }
     if (d->variant >= 11 && d->variant <= 13 && ring_row_aligned(d)) {
         const int st = d->variant == 11 ? 0 : (d->variant == 12 ? -1 : 1);
         if constexpr (sizeof(S) == 8) return launch_ring2_fp64(a, st, d->tile_y, s);
@@ -561,8 +569,8 @@ int sclbm_domain_step_rows(sclbm_domain *d, int row0, int nrows, int finish)
 int sclbm_domain_set_kernel(sclbm_domain *d, int variant, int tile_y)
 {
     if (!d) return set_error(SCLBM_E_INVALID_ARGUMENT, "null domain");
-    if (variant < 0 || variant > 13 || variant == 10)
-        return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0..9 or 11..13");
+    if (variant < 0 || variant > 14 || variant == 10)
+        return set_error(SCLBM_E_INVALID_ARGUMENT, "variant is 0..9 or 11..14");
     if (tile_y < 0 || tile_y > 4096) return set_error(SCLBM_E_INVALID_ARGUMENT, "bad tile_y");
     if (variant == 1 && !d->rho_tmp[0] && d->ncomp == 2) {
         const size_t es = d->prec == SCLBM_FP64 ? 8 : 4;

@@ -52,22 +52,30 @@ constexpr int RING_WAIT_LIMIT = 1 << 20; // polls of one stage before giving up 
 // elements per 16 bytes of storage type S
 template <typename S> constexpr int ring_pad() { return 16 / (int)sizeof(S); }
 
-template <typename S, typename T, int R, int W = RING_W> struct RingLayout {
+// HB: each stage holds the halo boxes of strips at the lattice's left and
+// right edges (the wrapped halo column).  Without them (4- and 8-byte storage
+// only) a stage is 1 KB smaller and the halo lane of such a strip copies the
+// wrapped column's populations of the next row into its own slot of a small
+// edge buffer (two slots per halo lane: 36 elements).
+template <typename S, typename T, int R, int W = RING_W, bool HB = true> struct RingLayout {
     static constexpr int A = ring_pad<S>();
     static constexpr int P = W + 2 * A; // box columns
     static constexpr int Q = W + 2;     // density ring columns
     // tensor-copy destinations start on 128-byte boundaries
     static constexpr size_t comp = (size_t(9) * P * sizeof(S) + 127) & ~size_t(127);
     static constexpr size_t halo = 256; // one A-column box of one component (144 bytes)
-    static constexpr size_t stage = 2 * comp + 4 * halo; // components, then halos [side][k]
+    static constexpr size_t stage = 2 * comp + (HB ? 4 * halo : 0); // components, then halos [side][k]
     static constexpr size_t pops = size_t(R) * stage;
     static constexpr size_t rho = size_t(4) * Q * sizeof(V2<T>);
     static constexpr size_t msk = size_t(4) * Q;
-    static constexpr size_t bars = (pops + rho + msk + 15) & ~size_t(15);
+    static constexpr size_t edge_at = (pops + rho + msk + 15) & ~size_t(15);
+    static constexpr size_t edge = HB ? 0 : size_t(2) * 2 * 18 * sizeof(S); // [slot][lane][k][i]
+    static constexpr size_t bars = (edge_at + edge + 15) & ~size_t(15);
     static constexpr size_t bytes = bars + size_t(R) * 8 + 16 + 128; // + base alignment
     static constexpr uint32_t CE = (uint32_t)(comp / sizeof(S));     // component stride, elements
     static_assert(comp % 128 == 0 && stage % 128 == 0, "tensor-copy alignment");
     static_assert(size_t(9) * A * sizeof(S) <= halo, "halo box");
+    static_assert(HB || sizeof(S) >= 4, "edge copies move 4 or 8 bytes");
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
@@ -99,6 +107,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
                  : "memory");
     return ok != 0;
 }
+// asynchronous copy of one 4- or 8-byte element from global into shared
+// memory (cp.async); only the issuing thread waits on it and reads it
+template <int B> __device__ __forceinline__ void cp_async_elem(uint32_t dst, const void *src)
+{
+    static_assert(B == 4 || B == 8, "cp.async.ca moves 4, 8 or 16 bytes");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(dst), "l"(src), "n"(B) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // one 3-D box of a tiled tensor map into shared memory (dst 128-byte aligned),
 // completing on mbarrier `bar`; coordinates in elements (x may be negative or
 // past the end: those elements arrive as zeros); no multicast
@@ -125,30 +143,33 @@ struct RingMaps {
 
 // resident CTAs per SM the register cap aims at (the ring's shared memory
 // allows about as many): the register tile's figures, six for FP32
-// arithmetic (five in the uniform solid form, which spills at 80 registers),
-// three for FP64
-template <typename T, int FLAGS> constexpr int ring_min_ctas()
+// arithmetic (five in the uniform solid form, which spills at 80 registers,
+// and without halo boxes, whose edge lanes hold a row of the wrapped column
+// in registers), three for FP64
+template <typename T, int FLAGS, bool HB = true> constexpr int ring_min_ctas()
 {
-    return sizeof(T) == 8 ? 3 : ((FLAGS & KF_UNIFORM) ? 5 : 6);
+    return sizeof(T) == 8 ? 3 : (((FLAGS & KF_UNIFORM) || !HB) ? 5 : 6);
 }
 
 // The shared-memory pieces of one CTA's ring.
-template <typename S, typename T, int R, int W = RING_W> struct RingShared {
+template <typename S, typename T, int R, int W = RING_W, bool HB = true> struct RingShared {
     unsigned char *base; // 128-byte aligned: the R stages
     V2<T> *rho;          // density ring [4][Q]
     uint8_t *msk;        // mask ring [4][Q]
+    S *edge;             // edge buffer (HB false)
     uint64_t *bars;      // one mbarrier per stage
     volatile int *abort_flag;
 };
 
-template <typename S, typename T, int R, int W = RING_W>
-__device__ __forceinline__ RingShared<S, T, R, W> ring_shared(unsigned char *raw)
+template <typename S, typename T, int R, int W = RING_W, bool HB = true>
+__device__ __forceinline__ RingShared<S, T, R, W, HB> ring_shared(unsigned char *raw)
 {
-    using L = RingLayout<S, T, R, W>;
-    RingShared<S, T, R, W> sh;
+    using L = RingLayout<S, T, R, W, HB>;
+    RingShared<S, T, R, W, HB> sh;
     sh.base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(raw) + 127) & ~uintptr_t(127));
     sh.rho = reinterpret_cast<V2<T> *>(sh.base + L::pops);
     sh.msk = sh.base + L::pops + L::rho;
+    sh.edge = reinterpret_cast<S *>(sh.base + L::edge_at);
     sh.bars = reinterpret_cast<uint64_t *>(sh.base + L::bars);
     sh.abort_flag = reinterpret_cast<volatile int *>(sh.base + L::bars + R * 8);
     if (threadIdx.x == 0) {
@@ -166,14 +187,14 @@ __device__ __forceinline__ RingShared<S, T, R, W> ring_shared(unsigned char *raw
 // stage's mbarrier phase follows from that count.  maps: row boxes of both
 // components, then halo boxes.  Returns false once the CTA has given up on a
 // bounded wait (*a.status is then set).
-template <typename S, typename T, int FLAGS, int R, bool WIDE, int W = RING_W>
+template <typename S, typename T, int FLAGS, int R, bool WIDE, int W = RING_W, bool HB = true>
 __device__ __forceinline__ bool ring_unit(const Fused2Args<S, T> &a, const CUtensorMap *map_row0,
                                           const CUtensorMap *map_row1, const CUtensorMap *map_halo0,
                                           const CUtensorMap *map_halo1, const int xb, const int y0,
-                                          const int nrow, const bool down, const RingShared<S, T, R, W> &sh,
-                                          uint32_t &g0)
+                                          const int nrow, const bool down,
+                                          const RingShared<S, T, R, W, HB> &sh, uint32_t &g0)
 {
-    using L = RingLayout<S, T, R, W>;
+    using L = RingLayout<S, T, R, W, HB>;
     constexpr int A = L::A, P = L::P, Q = L::Q;
     constexpr uint32_t CE = L::CE;
     constexpr bool SOLID = (FLAGS & KF_SOLID) != 0;
@@ -206,7 +227,8 @@ __device__ __forceinline__ bool ring_unit(const Fused2Args<S, T> &a, const CUten
     const bool wrap_l = xb == 0, wrap_r = xb + ncol == nx;
     const uint32_t box_bytes = 9u * (uint32_t)P * (uint32_t)sizeof(S);
     const uint32_t halo_bytes = 9u * (uint32_t)A * (uint32_t)sizeof(S);
-    const uint32_t row_bytes = 2u * (box_bytes + (wrap_l ? halo_bytes : 0u) + (wrap_r ? halo_bytes : 0u));
+    const uint32_t row_bytes =
+        2u * (box_bytes + (HB && wrap_l ? halo_bytes : 0u) + (HB && wrap_r ? halo_bytes : 0u));
     auto stage_at = [&](int st) { return ring_smem + (size_t)st * L::stage; };
     // lane 0 of warp 0 requests row j: one box per component (+ halo boxes)
     auto issue = [&](int j) {
@@ -220,10 +242,10 @@ __device__ __forceinline__ bool ring_unit(const Fused2Args<S, T> &a, const CUten
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
             tensor_g2s_3d(sb + k * (uint32_t)L::comp, rowm[k], xb - A, y, 0, bar);
-            if (wrap_l)
+            if (HB && wrap_l)
                 tensor_g2s_3d(sb + 2 * (uint32_t)L::comp + (0 + k) * (uint32_t)L::halo, halom[k], nx - A, y,
                               0, bar);
-            if (wrap_r)
+            if (HB && wrap_r)
                 tensor_g2s_3d(sb + 2 * (uint32_t)L::comp + (2 + k) * (uint32_t)L::halo, halom[k], 0, y, 0,
                               bar);
         }
@@ -242,6 +264,28 @@ __device__ __forceinline__ bool ring_unit(const Fused2Args<S, T> &a, const CUten
             issue(j);
             issued = j;
         }
+
+    // without halo boxes, a halo lane (t = 0 or 1) whose column wraps around
+    // the lattice edge copies that column's populations of ring row j into
+    // edge slot j & 1 one row ahead; it alone waits on and reads its copies
+    const bool edge = !HB && hal && (hl ? wrap_l : wrap_r);
+    auto edge_slot = [&](int j) { return sh.edge + ((j & 1) * 2 + t) * 18; };
+    auto copy_edge = [&](int j) {
+        if constexpr (!HB) {
+            const uint32_t node = (uint32_t)gy(j) * (uint32_t)nx + (uint32_t)xh;
+            const uint32_t dst = smem_addr(edge_slot(j));
+#pragma unroll
+            for (int k = 0; k < 2; ++k)
+#pragma unroll
+                for (int i = 0; i < 9; ++i)
+                    cp_async_elem<(int)sizeof(S)>(dst + (uint32_t)((k * 9 + i) * sizeof(S)),
+                                                  a.fin[k] + elem<WIDE>(i, a.N, node));
+            cp_async_commit();
+        }
+    };
+    if constexpr (!HB) {
+        if (edge) copy_edge(0);
+    }
 
     // masks of the next row, loaded one row ahead
     uint8_t mn = 1, mnh = 1;
@@ -289,10 +333,20 @@ __device__ __forceinline__ bool ring_unit(const Fused2Args<S, T> &a, const CUten
                 if (act) {
                     load(stg, CE, P, A + t, cur);
                     density(cur, m, t + 1);
-                    if (hal) {
+                    if (!HB && edge) {
+                        cp_async_wait_all(); // row j's copies, issued one iteration ago
+                        const S *e = edge_slot(j);
+                        T h[2][9];
+#pragma unroll
+                        for (int k = 0; k < 2; ++k)
+#pragma unroll
+                            for (int i = 0; i < 9; ++i) h[k][i] = T(e[k * 9 + i]);
+                        density(h, mh, hl ? 0 : ncol + 1);
+                        if (j < last) copy_edge(j + 1);
+                    } else if (hal) {
                         // the halo column wrapped around a lattice edge comes
                         // from its own box, else from the row box
-                        const bool wrap = hl ? wrap_l : wrap_r;
+                        const bool wrap = HB && (hl ? wrap_l : wrap_r);
                         const S *hp = wrap ? (hl ? hlp : hrp) : stg;
                         const uint32_t hcs = wrap ? HE : CE;
                         const int hds = wrap ? A : P;
@@ -340,17 +394,20 @@ __device__ __forceinline__ bool ring_unit(const Fused2Args<S, T> &a, const CUten
         // let the copies still in flight land before the CTA's shared memory is released
         for (int j = consumed + 1; j <= issued; ++j) (void)wait_row(j);
     }
+    if constexpr (!HB) {
+        if (edge) cp_async_wait_all(); // an edge copy still in flight after an abort
+    }
     g0 = gbase + (uint32_t)(last + 1);
     return !aborted;
 }
 
 // One band of one strip per CTA; band b covers rows [b*ny/bands, (b+1)*ny/bands).
-template <typename S, typename T, int FLAGS, int R, bool WIDE>
-__global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS>()))
+template <typename S, typename T, int FLAGS, int R, bool WIDE, bool HB>
+__global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS, HB>()))
     k_ring2(const __grid_constant__ Fused2Args<S, T> a, const __grid_constant__ RingMaps maps, int bands)
 {
     extern __shared__ __align__(128) unsigned char ring_raw[];
-    const RingShared<S, T, R> sh = ring_shared<S, T, R>(ring_raw);
+    const RingShared<S, T, R, RING_W, HB> sh = ring_shared<S, T, R, RING_W, HB>(ring_raw);
     if (threadIdx.x == 0) {
         asm volatile("prefetch.tensormap [%0];" ::"l"(&maps.row[0]) : "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(&maps.row[1]) : "memory");
@@ -359,8 +416,9 @@ __global__ void __launch_bounds__(RING_W, (ring_min_ctas<T, FLAGS>()))
     const int y0 = (int)((long long)band * a.ny / bands);
     const int nrow = (int)((long long)(band + 1) * a.ny / bands) - y0;
     uint32_t g = 0;
-    (void)ring_unit<S, T, FLAGS, R, WIDE>(a, &maps.row[0], &maps.row[1], &maps.halo[0], &maps.halo[1],
-                                          blockIdx.x * RING_W, y0, nrow, (band & 1) != 0, sh, g);
+    (void)ring_unit<S, T, FLAGS, R, WIDE, RING_W, HB>(a, &maps.row[0], &maps.row[1], &maps.halo[0],
+                                                      &maps.halo[1], blockIdx.x * RING_W, y0, nrow,
+                                                      (band & 1) != 0, sh, g);
 }
 
 // A unit of the batched ring kernel: strip xb of rows [y0, y1) of domain dom;
@@ -444,11 +502,11 @@ inline cudaError_t ring_maps(const Fused2Args<S, T> &a, RingMaps &m)
 // ran 5-25 % slower than 32-row bands, 128-row bands 3-14 % slower (FP32 and
 // FP64, disks of radius 8-20 at 60 % fluid and 2-8 at 72 %).
 constexpr int RING_ROWS = 32;
-template <typename S, typename T, int FLAGS, int R, bool WIDE>
+template <typename S, typename T, int FLAGS, int R, bool WIDE, bool HB>
 inline cudaError_t launch_ring2_f(const Fused2Args<S, T> &a, int rows, cudaStream_t s)
 {
-    using L = RingLayout<S, T, R>;
-    auto kern = k_ring2<S, T, FLAGS, R, WIDE>;
+    using L = RingLayout<S, T, R, RING_W, HB>;
+    auto kern = k_ring2<S, T, FLAGS, R, WIDE, HB>;
     static int per_sm = 0; // resident CTAs per SM of this instantiation (one device): >= 1 checked once
     if (per_sm == 0) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes);
@@ -475,17 +533,19 @@ inline cudaError_t launch_ring2_f(const Fused2Args<S, T> &a, int rows, cudaStrea
 // 16 / sizeof(S) (buffers from cudaMalloc are 256-byte aligned)
 template <typename S> inline bool ring_fits(int nx) { return nx % ring_pad<S>() == 0; }
 
-// UNI: lattices with solid nodes run the uniform solid form (KF_UNIFORM)
-template <typename S, typename T, int R, int UNI = KF_UNIFORM>
+// UNI: lattices with solid nodes run the uniform solid form (KF_UNIFORM);
+// HB: halo boxes in the stages (else edge columns from global memory)
+template <typename S, typename T, int R, int UNI = KF_UNIFORM, bool HB = true>
 inline cudaError_t launch_ring2_any(const Fused2Args<S, T> &a, int rows, cudaStream_t s)
 {
     if (!ring_fits<S>(a.nx) || a.nx < 1 || a.ny < 1) return cudaErrorInvalidValue;
-    if (needs_wide_offsets(a.N)) return launch_ring2_f<S, T, KF_FORCE | KF_SOLID | UNI, R, true>(a, rows, s);
+    if (needs_wide_offsets(a.N))
+        return launch_ring2_f<S, T, KF_FORCE | KF_SOLID | UNI, R, true, HB>(a, rows, s);
     switch (kernel_flags(a)) {
-    case 0: return launch_ring2_f<S, T, 0, R, false>(a, rows, s);
-    case KF_FORCE: return launch_ring2_f<S, T, KF_FORCE, R, false>(a, rows, s);
-    case KF_SOLID: return launch_ring2_f<S, T, KF_SOLID | UNI, R, false>(a, rows, s);
-    default: return launch_ring2_f<S, T, KF_FORCE | KF_SOLID | UNI, R, false>(a, rows, s);
+    case 0: return launch_ring2_f<S, T, 0, R, false, HB>(a, rows, s);
+    case KF_FORCE: return launch_ring2_f<S, T, KF_FORCE, R, false, HB>(a, rows, s);
+    case KF_SOLID: return launch_ring2_f<S, T, KF_SOLID | UNI, R, false, HB>(a, rows, s);
+    default: return launch_ring2_f<S, T, KF_FORCE | KF_SOLID | UNI, R, false, HB>(a, rows, s);
     }
 }
 

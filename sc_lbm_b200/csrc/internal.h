@@ -166,9 +166,14 @@ cudaError_t launch_batch2_async_f32(const Fused2Args<float, float> *doms, const 
 // by tensor copies; stages selects the ring depth (0 default, -1 fewer, +1
 // more), rows the rows per band (0 default); cudaErrorInvalidValue when nx is
 // not a multiple of 16 / sizeof(storage)
-cudaError_t launch_ring2_fp64(const Fused2Args<double, double> &a, int stages, int rows, cudaStream_t s);
-cudaError_t launch_ring2_f32(const Fused2Args<float, float> &a, int stages, int rows, cudaStream_t s);
-cudaError_t launch_ring2_f16(const Fused2Args<__half, float> &a, int stages, int rows, cudaStream_t s);
+// edge: the default depth (stages -1 for FP64 and FP16, +1 for FP32)
+// without halo boxes in the stages (lattice-edge columns from global memory)
+cudaError_t launch_ring2_fp64(const Fused2Args<double, double> &a, int stages, int rows, cudaStream_t s,
+                              bool edge = false);
+cudaError_t launch_ring2_f32(const Fused2Args<float, float> &a, int stages, int rows, cudaStream_t s,
+                             bool edge = false);
+cudaError_t launch_ring2_f16(const Fused2Args<__half, float> &a, int stages, int rows, cudaStream_t s,
+                             bool edge = false);
 // batched ring kernel (fused_ring.cuh): maps and units are device arrays
 // (RingMaps per domain and parity; RingUnit work list); counters: two
 // device words, zero before the first launch

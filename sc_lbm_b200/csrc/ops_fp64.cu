@@ -438,8 +438,11 @@ int async_resident_fp64() { return async_resident_ctas<double, double, 128, 3>()
 // lanes branch around the collision as in the FP64 register tile
 #include "fused_ring.cuh"
 namespace sclbm {
-cudaError_t launch_ring2_fp64(const Fused2Args<double, double> &a, int stages, int rows, cudaStream_t s)
+cudaError_t launch_ring2_fp64(const Fused2Args<double, double> &a, int stages, int rows, cudaStream_t s,
+                              bool edge)
 {
+    // FP64 keeps its halo boxes: its registers, not its stages, set its residency
+    if (edge) return launch_ring2_any<double, double, 2, 0>(a, rows, s);
     if (stages < 0) return launch_ring2_any<double, double, 2, 0>(a, rows, s);
     if (stages > 0) return launch_ring2_any<double, double, 4, 0>(a, rows, s);
     return launch_ring2_any<double, double, 3, 0>(a, rows, s);

@@ -100,16 +100,23 @@ int batch_blocks_per_sm(sclbm_precision p, int body)
 
 #include "fused_ring.cuh"
 namespace sclbm {
-// FP32: 9.8 KB per stage; three stages (34 KB) keep the six CTAs per SM that
-// the registers allow.  FP16: 5.2 KB per stage, five stages.
-cudaError_t launch_ring2_f32(const Fused2Args<float, float> &a, int stages, int rows, cudaStream_t s)
+// FP32: 10.8 KB per stage with halo boxes (9.8 KB without); FP16: 6.3 KB
+// (5.3 KB).  Without halo boxes four FP32 stages leave room for five CTAs per
+// SM instead of four.
+cudaError_t launch_ring2_f32(const Fused2Args<float, float> &a, int stages, int rows, cudaStream_t s,
+                             bool edge)
 {
+    if (edge) return launch_ring2_any<float, float, 4, KF_UNIFORM, false>(a, rows, s);
     if (stages < 0) return launch_ring2_any<float, float, 2>(a, rows, s);
     if (stages > 0) return launch_ring2_any<float, float, 4>(a, rows, s);
     return launch_ring2_any<float, float, 3>(a, rows, s);
 }
-cudaError_t launch_ring2_f16(const Fused2Args<__half, float> &a, int stages, int rows, cudaStream_t s)
+cudaError_t launch_ring2_f16(const Fused2Args<__half, float> &a, int stages, int rows, cudaStream_t s,
+                             bool edge)
 {
+    // FP16 keeps its halo boxes: its registers set its residency, and its
+    // 2-byte elements are below the smallest asynchronous element copy
+    if (edge) return launch_ring2_any<__half, float, 4>(a, rows, s);
     if (stages < 0) return launch_ring2_any<__half, float, 4>(a, rows, s);
     if (stages > 0) return launch_ring2_any<__half, float, 6>(a, rows, s);
     return launch_ring2_any<__half, float, 5>(a, rows, s);

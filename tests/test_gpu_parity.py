@@ -73,7 +73,7 @@ def test_domain_fp64_bit_exact(sclbm, name):
                                                (128, 3, 4), (128, 0, 5), (128, 4, 5),
                                                (128, 0, 7), (128, 0, 8), (128, 3, 8),
                                                (128, 0, 9), (32, 0, 2), (32, 5, 8), (32, 4, 1),
-                                               (128, 0, 11), (128, 0, 12), (128, 0, 13)])
+                                               (128, 0, 11), (128, 0, 12), (128, 0, 13), (128, 0, 14)])
 def test_domain_fp64_tiling_invariant(sclbm, tx, tile_y, variant):
     """Kernel variant (pipelined persistent, two pass, register tile, register
     tile with L2 prefetch, ring of bulk row copies at three depths) and tile
@@ -190,7 +190,8 @@ def test_shifted_forms_close_each_nodes_mass(sclbm):
                                                (6, 0, 128), (6, 1, 128), (6, 5, 128), (6, 64, 128),
                                                (7, 0, 128), (7, 3, 128), (8, 0, 128), (8, 5, 128),
                                                (9, 0, 128), (0, 0, 32), (2, 3, 32), (8, 7, 32),
-                                               (11, 0, 128), (12, 0, 128), (13, 0, 128)])
+                                               (11, 0, 128), (12, 0, 128), (13, 0, 128), (14, 0, 128),
+                                               (14, 5, 128)])
 def test_shifted_variants_match_register_tile(sclbm, variant, tile_y, tx):
     """The shifted forms give the same bytes with every kernel variant and
     tile width."""
@@ -213,35 +214,40 @@ RING_LATTICES = [(8, 3, []), (136, 20, [("walls", 1, "x")]), (264, 9, [("circle"
                  (256, 33, [("circle", 9, 200, 16), ("walls", 1, "x")])]
 
 
+@pytest.mark.parametrize("variant", [11, 14])
 @pytest.mark.parametrize("nx,ny,geom", RING_LATTICES)
-def test_ring_kernel_ragged_lattices(sclbm, oracle, nx, ny, geom):
-    """Ring kernel (variant 11) on awkward shapes: FP64 bit for bit with the
-    oracle, FP32/FP16 byte for byte with the register tile."""
+def test_ring_kernel_ragged_lattices(sclbm, oracle, nx, ny, geom, variant):
+    """Ring kernel on awkward shapes, with halo boxes in its stages (variant
+    11) and with the lattice-edge columns copied from global memory (variant
+    14, FP32): FP64 bit for bit with the oracle, FP32/FP16 byte for byte with
+    the register tile."""
     f = np.concatenate([cases.noisy_f_equilibrium(nx + 3 * ny, nx, ny, 1.0, 0.02, 0.03),
                         cases.noisy_f_equilibrium(nx + 5 * ny, nx, ny, 0.4, 0.02, 0.03)])
     case = dict(nx=nx, ny=ny, geom=geom, mode="two", fluid1=(0.9, 1.1, 0.1),
                 fluid2=(1.2, 1.1, -0.1), init=("file", f),
                 force=(3, cases.force_vec(1e-4, "x")), steps=9)
     want = oracle.run_case(case)
-    got = gpu_runner.run_domain(sclbm, case, sclbm.FP64, variant=11)
+    got = gpu_runner.run_domain(sclbm, case, sclbm.FP64, variant=variant)
     for k in ("c1_f", "c2_f", "c1_rho_final", "c2_ux_final"):
         assert got[k].tobytes() == want[k].tobytes(), (nx, ny, k)
     got["_domain"].mass_momentum()
     for prec in (sclbm.FP32_SHIFTED, sclbm.FP16_SHIFTED):
         a = gpu_runner.run_domain(sclbm, case, prec, rho_ref=(1.0, 0.4))
-        b = gpu_runner.run_domain(sclbm, case, prec, rho_ref=(1.0, 0.4), variant=11)
+        b = gpu_runner.run_domain(sclbm, case, prec, rho_ref=(1.0, 0.4), variant=variant)
         assert a["c1_f"].tobytes() == b["c1_f"].tobytes(), (nx, ny, prec)
         assert a["c2_f"].tobytes() == b["c2_f"].tobytes(), (nx, ny, prec)
         b["_domain"].mass_momentum()
 
 
-@pytest.mark.parametrize("prec_name,ny,porous", [("FP64", 1024, False), ("FP32_SHIFTED", 1536, False),
-                                                 ("FP32_SHIFTED", 1536, True), ("FP16_SHIFTED", 2048, False)])
-def test_default_kernel_on_lattices_that_fill_the_gpu(sclbm, prec_name, ny, porous):
+@pytest.mark.parametrize("prec_name,ny,porous,variant", [
+    ("FP64", 1024, False, 0), ("FP32_SHIFTED", 1536, False, 0), ("FP32_SHIFTED", 1536, True, 0),
+    ("FP16_SHIFTED", 2048, False, 0), ("FP32_SHIFTED", 1536, False, 14), ("FP32_SHIFTED", 1536, True, 14)])
+def test_default_kernel_on_lattices_that_fill_the_gpu(sclbm, prec_name, ny, porous, variant):
     """Lattices large enough for the default kernel choice to take the ring
     (4096 wide, 2048 bands of the precision's default height: 16 rows FP64, 24
     FP32, 32 FP16) give the register tile's populations byte for byte after
-    three steps, all-fluid and porous with a volume force."""
+    three steps, all-fluid and porous with a volume force; so does the FP32
+    ring without halo boxes (variant 14), five CTAs per SM."""
     from sc_lbm_b200 import workloads as W
     prec = getattr(sclbm, prec_name)
     nx = 4096
@@ -252,9 +258,9 @@ def test_default_kernel_on_lattices_that_fill_the_gpu(sclbm, prec_name, ny, poro
     params = sclbm.make_params(ncomp=2, tau=(0.9, 1.1), g_fluid=(1.2, 1.2), g_solid=(-0.2, 0.2),
                                rho_ref=(1.0, 1.0), force=(cases.force_vec(1e-5, "x") if porous else None, None))
     digests = []
-    for variant in (0, 2):
+    for v in (variant, 2):
         d = sclbm.Domain(nx, ny, mask, params, prec)
-        d.set_kernel(variant, 0)
+        d.set_kernel(v, 0)
         d.init_noise(0, 1.0, 0.02, 5)
         d.init_noise(1, 1.0, 0.02, 6)
         d.step(3)

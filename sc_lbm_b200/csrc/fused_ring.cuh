@@ -211,9 +211,14 @@ __device__ __forceinline__ bool ring_unit(const Fused2Args<S, T> &a, const CUten
     const int x = act ? xb + t : xb;
     const int xl = wrap1(x - 1, nx), xr = wrap1(x + 1, nx);
     // the densities of the two halo columns come from lanes 0 (left) and 1
-    // (right) of warp 0, which run the same instructions side by side (ncol >= 2:
-    // rows hold a multiple of A >= 2 nodes)
-    const bool hl = t == 0, hal = t <= 1;
+    // (right) of warp HW, which run the same instructions side by side whether
+    // or not their own columns hold nodes.  FP16 storage takes them to warp 1,
+    // away from warp 0, which issues the row copies: its issue-bound rows then
+    // wait less at the row barrier (4096^2: 49.1 -> 50.3 GLUPS all-fluid,
+    // 37.4 -> 38.2 at 72 % fluid); FP32 storage ran 1.2 % slower that way
+    // (41.1 -> 40.6) and keeps them in warp 0, as does FP64 (no change)
+    constexpr int HW = (sizeof(S) == 2 && W >= 64) ? 1 : 0;
+    const bool hal = warp == HW && lane <= 1, hl = hal && lane == 0;
     const int xh = hl ? wrap1(xb - 1, nx) : wrap1(xb + ncol, nx);
     const int last = nrow + 1;
     const uint32_t gbase = g0;
@@ -265,11 +270,11 @@ __device__ __forceinline__ bool ring_unit(const Fused2Args<S, T> &a, const CUten
             issued = j;
         }
 
-    // without halo boxes, a halo lane (t = 0 or 1) whose column wraps around
-    // the lattice edge copies that column's populations of ring row j into
-    // edge slot j & 1 one row ahead; it alone waits on and reads its copies
+    // without halo boxes, a halo lane whose column wraps around the lattice
+    // edge copies that column's populations of ring row j into its edge slot
+    // j & 1 one row ahead; it alone waits on and reads its copies
     const bool edge = !HB && hal && (hl ? wrap_l : wrap_r);
-    auto edge_slot = [&](int j) { return sh.edge + ((j & 1) * 2 + t) * 18; };
+    auto edge_slot = [&](int j) { return sh.edge + ((j & 1) * 2 + (hl ? 0 : 1)) * 18; };
     auto copy_edge = [&](int j) {
         if constexpr (!HB) {
             const uint32_t node = (uint32_t)gy(j) * (uint32_t)nx + (uint32_t)xh;
@@ -289,9 +294,9 @@ __device__ __forceinline__ bool ring_unit(const Fused2Args<S, T> &a, const CUten
 
     // masks of the next row, loaded one row ahead
     uint8_t mn = 1, mnh = 1;
-    if (SOLID && act) {
+    if (SOLID) {
         const size_t row = (size_t)gy(0) * (size_t)nx;
-        mn = a.mask[row + x];
+        if (act) mn = a.mask[row + x];
         if (hal) mnh = a.mask[row + xh];
     }
     bool aborted = false;
@@ -302,9 +307,9 @@ __device__ __forceinline__ bool ring_unit(const Fused2Args<S, T> &a, const CUten
     // collide row j - 1 (prev) from the stencil rows j - 2, j - 1, j
     auto step_row = [&](const int j, T(&cur)[2][9], const T(&prev)[2][9]) {
         const uint8_t m = mn, mh = mnh;
-        if (SOLID && act && j < last) {
+        if (SOLID && j < last) {
             const size_t row = (size_t)gy(j + 1) * (size_t)nx;
-            mn = a.mask[row + x];
+            if (act) mn = a.mask[row + x];
             if (hal) mnh = a.mask[row + xh];
         }
         const int slot = j & 3;
@@ -333,28 +338,28 @@ __device__ __forceinline__ bool ring_unit(const Fused2Args<S, T> &a, const CUten
                 if (act) {
                     load(stg, CE, P, A + t, cur);
                     density(cur, m, t + 1);
-                    if (!HB && edge) {
-                        cp_async_wait_all(); // row j's copies, issued one iteration ago
-                        const S *e = edge_slot(j);
-                        T h[2][9];
+                }
+                if (!HB && edge) {
+                    cp_async_wait_all(); // row j's copies, issued one iteration ago
+                    const S *e = edge_slot(j);
+                    T h[2][9];
 #pragma unroll
-                        for (int k = 0; k < 2; ++k)
+                    for (int k = 0; k < 2; ++k)
 #pragma unroll
-                            for (int i = 0; i < 9; ++i) h[k][i] = T(e[k * 9 + i]);
-                        density(h, mh, hl ? 0 : ncol + 1);
-                        if (j < last) copy_edge(j + 1);
-                    } else if (hal) {
-                        // the halo column wrapped around a lattice edge comes
-                        // from its own box, else from the row box
-                        const bool wrap = HB && (hl ? wrap_l : wrap_r);
-                        const S *hp = wrap ? (hl ? hlp : hrp) : stg;
-                        const uint32_t hcs = wrap ? HE : CE;
-                        const int hds = wrap ? A : P;
-                        const int hcol = wrap ? (hl ? A - 1 : 0) : (hl ? A - 1 : A + ncol);
-                        T h[2][9];
-                        load(hp, hcs, hds, hcol, h);
-                        density(h, mh, hl ? 0 : ncol + 1);
-                    }
+                        for (int i = 0; i < 9; ++i) h[k][i] = T(e[k * 9 + i]);
+                    density(h, mh, hl ? 0 : ncol + 1);
+                    if (j < last) copy_edge(j + 1);
+                } else if (hal) {
+                    // the halo column wrapped around a lattice edge comes
+                    // from its own box, else from the row box
+                    const bool wrap = HB && (hl ? wrap_l : wrap_r);
+                    const S *hp = wrap ? (hl ? hlp : hrp) : stg;
+                    const uint32_t hcs = wrap ? HE : CE;
+                    const int hds = wrap ? A : P;
+                    const int hcol = wrap ? (hl ? A - 1 : 0) : (hl ? A - 1 : A + ncol);
+                    T h[2][9];
+                    load(hp, hcs, hds, hcol, h);
+                    density(h, mh, hl ? 0 : ncol + 1);
                 }
             } else {
                 *abort_flag = 1;

@@ -26,7 +26,8 @@
 // (a box's first column must start on a 16-byte boundary: nx must be a
 // multiple of A).  Columns outside the lattice arrive as zeros; where a strip
 // touches the lattice's left or right edge, the periodic halo column comes
-// from a second, A-column box at the other edge.
+// from a second, A-column box at the other edge (or, in the form without
+// halo boxes, from element copies into a small edge buffer one row ahead).
 // Iteration j waits for row j, reads each thread's column into registers and
 // reduces it to both components' densities (density ring in shared memory,
 // one __syncthreads); the stage is then free and is refilled at once with row

@@ -309,7 +309,7 @@ static bool ring_row_aligned(const sclbm_domain *d)
 //   FP32  4 stages, 24 rows: 41.6 (16 rows 41.3, 32 rows 40.1; 3 stages 36.8;
 //         5 stages 37.5; register tile 37.6) / 33.1 at 16 rows, 32.9 at 32
 //   FP16  4 stages, 32 rows: 49.4 / 35.6 (5 stages 49.0 / 35.3; register tile
-//         47.6 / 35.2)
+//         47.6 / 35.2); 50.3 / 38.2 since its halo columns are reduced by warp 1
 struct RingChoice {
     int stages, rows;
 };

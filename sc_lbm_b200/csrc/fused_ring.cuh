@@ -145,8 +145,8 @@ struct RingMaps {
 // resident CTAs per SM the register cap aims at (the ring's shared memory
 // allows about as many): the register tile's figures, six for FP32
 // arithmetic (five in the uniform solid form, which spills at 80 registers,
-// and without halo boxes, whose edge lanes hold a row of the wrapped column
-// in registers), three for FP64
+// and without halo boxes, whose smaller stages let a fifth CTA's shared
+// memory fit), three for FP64
 template <typename T, int FLAGS, bool HB = true> constexpr int ring_min_ctas()
 {
     return sizeof(T) == 8 ? 3 : (((FLAGS & KF_UNIFORM) || !HB) ? 5 : 6);
